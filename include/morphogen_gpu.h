@@ -1,0 +1,157 @@
+/*
+ * morphogen_gpu.h -- C ABI of the B200 (sm_100a) per-server PIR answer path.
+ *
+ * One server holds a table of `rows` rows of `row_bytes` bytes (row_bytes a
+ * multiple of 16, at most 4096) resident in HBM.  A query key is a ChaCha8
+ * GGM DPF key share in the reference's unchanged wire format
+ * (ChaChaKey::to_bytes, crates/morphogen-gpu-dpf/src/dpf.rs:259-274).  The
+ * server's answer share for a key is
+ *
+ *     share = XOR_{i < rows} ( row_i AND mask(i) ),  mask(i) = key.eval(i)
+ *
+ * with the 16-byte DPF output repeated over every 16-byte lane of the row
+ * (crates/morphogen-gpu-dpf/src/kernel.rs:1243-1256, generalised from 4096-B
+ * pages to R-byte rows; the reference's page mode is row_bytes = 4096).
+ *
+ * All entry points use C linkage, plain pointers and sizes, return an int
+ * status (MG_OK == 0) and never throw.  mg_last_error() returns a
+ * thread-local message for the last failing call on the calling thread.
+ * A context may be used from several host threads: calls on one context are
+ * serialised internally; distinct mg_batch workspaces may be driven from
+ * different threads and overlap on the device through their own streams.
+ */
+#ifndef MORPHOGEN_GPU_H
+#define MORPHOGEN_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference surfaces DriverError (mapped to HTTP 500) and
+ * GpuDpfError (crates/morphogen-gpu-dpf/src/dpf.rs:9-15). */
+enum {
+  MG_OK = 0,
+  MG_EINVAL = 1,    /* bad argument (null pointer, row_bytes % 16 != 0, ...)    */
+  MG_EKEY = 2,      /* malformed key bytes: GpuDpfError::InvalidKeyFormat       */
+  MG_ERANGE = 3,    /* index beyond the DPF domain: PageIndexTooLarge, or more
+                       rows than 2^domain_bits (kernel.rs:1283-1285)             */
+  MG_ENOMEM = 4,    /* device or pinned-host allocation failed                  */
+  MG_ECUDA = 5,     /* CUDA runtime error: DriverError                          */
+  MG_ETIMEDOUT = 6, /* the pass did not complete before the caller's deadline   */
+  MG_ENODEV = 7,    /* no usable sm_100 device                                  */
+  MG_EBUSY = 8      /* workspace still owns a pass in flight                    */
+};
+
+/* Largest DPF depth the device path accepts.  ChaChaParams::new allows up to
+ * 32 levels (dpf.rs:65-79); the reference kernel silently truncates at 25
+ * (kernel.rs:45,131-136), this library evaluates all 32. */
+#define MG_MAX_DOMAIN_BITS 32
+#define MG_MAX_ROW_BYTES 4096
+
+typedef struct mg_context mg_context; /* GpuScanner                      */
+typedef struct mg_table mg_table;     /* GpuPageMatrix with R-byte rows  */
+typedef struct mg_batch mg_batch;     /* BatchWorkspace (kernel.rs:163-171) */
+
+/* KernelTiming (kernel.rs:1214-1228); whole-pass figures in nanoseconds. */
+typedef struct {
+  uint64_t h2d_ns;
+  uint64_t kernel_ns; /* CUDA-event time of the scan + reduction kernels */
+  uint64_t d2h_ns;
+  uint64_t total_ns;
+} mg_timing;
+
+/* Launch shape chosen for a pass (the autotuner's decision). */
+typedef struct {
+  uint32_t subtree_bits;  /* leaves per work item = 2^subtree_bits (largest segment) */
+  uint32_t keys_per_cta;  /* keys evaluated together on one row tile */
+  uint32_t grid;          /* persistent CTAs launched */
+  uint32_t items;         /* (tile, key group) work items */
+  uint32_t segments;      /* (table, domain) segments in the pass */
+  uint32_t smem_bytes;    /* dynamic shared memory per CTA */
+} mg_plan_info;
+
+/* ---- context: GpuScanner::new (kernel.rs:258-465) ------------------------ */
+int mg_context_create(int device, mg_context** out);
+int mg_context_destroy(mg_context* ctx);
+const char* mg_last_error(void);
+/* SM count and free/total device memory (admission control). */
+int mg_device_info(mg_context* ctx, int* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* ---- tables: GpuPageMatrix (crates/morphogen-gpu-dpf/src/storage.rs) ------ */
+/* alloc_empty (storage.rs:89-101): zero-filled rows x row_bytes on the device. */
+int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table** out);
+int mg_table_destroy(mg_table* table);
+/* update_pages (storage.rs:104-124) / new (storage.rs:27-43): host -> device. */
+int mg_table_write_rows(mg_table* table, uint64_t first_row, const void* host_rows, uint64_t nrows);
+int mg_table_read_rows(const mg_table* table, uint64_t first_row, void* host_rows, uint64_t nrows);
+/* Synthetic content: byte o = byte (o % 8) of SplitMix64 output o / 8 of the
+ * stream seeded with `seed`; generated on the device. */
+int mg_table_fill_splitmix(mg_table* table, uint64_t seed);
+/* Epoch merge: row_idx[i] ^= diffs[i] for n entries, in place on the device
+ * (the GPU half of EpochManager::try_advance, server/epoch.rs:516-545, and
+ * the XOR patch of try_build_snapshot_from_entries, server/epoch.rs:118-181).
+ * Host arrays; row indices must be < rows. */
+int mg_table_xor_rows(mg_table* table, const uint64_t* row_idx, const void* diffs, uint64_t n);
+uint64_t mg_table_rows(const mg_table* table);
+uint32_t mg_table_row_bytes(const mg_table* table);
+const void* mg_table_device_ptr(const mg_table* table);
+
+/* ---- keys: ChaChaKey (crates/morphogen-gpu-dpf/src/dpf.rs) ---------------- */
+/* Wire length 19 + 18 d + 16 (dpf.rs:287). */
+size_t mg_key_size(uint32_t domain_bits);
+/* ChaChaKey::from_bytes validation (dpf.rs:277-316) plus d <= 32. */
+int mg_key_check(const uint8_t* key, size_t len, uint32_t* domain_bits, uint8_t* party);
+/* generate_chacha_dpf_keys (dpf.rs:322-432) with caller-supplied root seeds
+ * (the reference draws them from rand::random, dpf.rs:332-333).  key0/key1
+ * must each hold mg_key_size(domain_bits) bytes. */
+int mg_keygen(uint32_t domain_bits, uint64_t target, const uint8_t root_seed0[16],
+              const uint8_t root_seed1[16], uint8_t* key0, uint8_t* key1);
+
+/* ---- one-call scan: GpuScanner::scan / scan_batch (kernel.rs:685-935) ----- */
+/* Evaluates nkeys keys in one pass; key i is scanned over tables[i] (tables
+ * may repeat and may differ: mixed-size batching).  out_shares receives the
+ * shares back to back, share i being row_bytes(tables[i]) bytes.  Keys and
+ * shares are host memory; the copies are inside the call.  timeout_ms == 0
+ * waits without a deadline; otherwise MG_ETIMEDOUT is returned if the pass
+ * has not finished in time (the pass still completes on the device; the
+ * context's internal workspace stays busy until it does).  timing may be NULL. */
+int mg_scan(mg_context* ctx, const mg_table* const* tables, const uint8_t* const* keys,
+            const size_t* key_lens, uint32_t nkeys, uint8_t* out_shares, uint32_t timeout_ms,
+            mg_timing* timing);
+
+/* ---- workspaces: BatchWorkspace + scan_batch_opts (kernel.rs:163-171,711-924) */
+int mg_batch_create(mg_context* ctx, mg_batch** out);
+int mg_batch_destroy(mg_batch* batch);
+/* Parse and stage keys, plan the pass, copy the keys to the device on the
+ * workspace stream.  Reallocates device buffers only when they grow. */
+int mg_batch_set_keys(mg_batch* batch, const mg_table* const* tables, const uint8_t* const* keys,
+                      const size_t* key_lens, uint32_t nkeys);
+/* Pin the launch shape (0 = let the autotuner choose). */
+int mg_batch_set_shape(mg_batch* batch, uint32_t subtree_bits, uint32_t keys_per_cta);
+/* Enqueue the scan and reduction kernels on `stream` (a cudaStream_t; NULL =
+ * the workspace's own stream).  Keys and tables must already be resident.
+ * Launch-only: capturable into a CUDA graph by the caller. */
+int mg_batch_launch(mg_batch* batch, void* stream);
+/* Replay the pass from a CUDA graph captured on first use (same keys layout). */
+int mg_batch_launch_graph(mg_batch* batch, void* stream);
+/* Device -> host copy of the shares (enqueued on the stream; see mg_batch_sync). */
+int mg_batch_read(mg_batch* batch, uint8_t* out_shares, void* stream);
+/* Wait for the workspace stream with a deadline (0 = none). */
+int mg_batch_sync(mg_batch* batch, uint32_t timeout_ms);
+int mg_batch_shares_device(mg_batch* batch, const void** dptr, size_t* bytes);
+int mg_batch_plan(mg_batch* batch, mg_plan_info* info);
+/* Timing of the last completed launch on the workspace stream. */
+int mg_batch_last_kernel_ns(mg_batch* batch, uint64_t* ns);
+
+/* ---- point evaluation on the device: ChaChaKey::eval (dpf.rs:103-142) ----- */
+/* out: n * 16 bytes, out[i] = eval(idx[i]).  Host arrays. */
+int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const uint64_t* idx,
+                   uint64_t n, uint8_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MORPHOGEN_GPU_H */

@@ -1,0 +1,889 @@
+// mg_api.cu -- C ABI (include/morphogen_gpu.h) over the sm_100a kernels.
+//
+// Host-side counterpart of the reference's GpuScanner / GpuPageMatrix /
+// BatchWorkspace (crates/morphogen-gpu-dpf/src/{kernel,storage}.rs): key
+// parsing from the unchanged wire format, pass planning (segments of
+// (table, domain), key groups, tile depth), persistent device workspaces,
+// CUDA-graph replay, and host deadlines instead of unbounded waits.
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "mg_internal.h"
+#include "morphogen_gpu.h"
+
+using mg::KeyDev;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define MG_CUDA(expr)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess) return fail(MG_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---- host ChaCha8 PRG (keygen only; chacha_prg.rs:93-178) -------------------
+inline uint32_t hrotl(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
+
+void host_block(const uint32_t key[8], uint32_t ctr, uint32_t out[16]) {
+  uint32_t s[16] = {mg::kSigma0, mg::kSigma1, mg::kSigma2, mg::kSigma3, key[0], key[1], key[2],
+                    key[3],      key[4],      key[5],      key[6],      key[7], ctr,    0,
+                    0,           0};
+  uint32_t x[16];
+  std::memcpy(x, s, sizeof s);
+  auto qr = [&](int a, int b, int c, int d) {
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = hrotl(x[d], 16);
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = hrotl(x[b], 12);
+    x[a] += x[b]; x[d] ^= x[a]; x[d] = hrotl(x[d], 8);
+    x[c] += x[d]; x[b] ^= x[c]; x[b] = hrotl(x[b], 7);
+  };
+  for (int r = 0; r < 4; ++r) {
+    qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
+    qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
+  }
+  for (int i = 0; i < 16; ++i) out[i] = x[i] + s[i];
+}
+
+void host_expand(const uint32_t seed[4], uint32_t L[4], uint32_t R[4], uint8_t& lt, uint8_t& rt) {
+  const uint32_t key[8] = {seed[0], seed[1], seed[2], seed[3], seed[0], seed[1], seed[2], seed[3]};
+  uint32_t b0[16], b1[16];
+  host_block(key, 0, b0);
+  host_block(key, 1, b1);
+  for (int i = 0; i < 4; ++i) { L[i] = b0[i]; R[i] = b0[4 + i]; }
+  lt = (uint8_t)(b1[0] & 1u);
+  rt = (uint8_t)(b1[1] & 1u);
+}
+
+inline uint32_t le32(const uint8_t* p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+inline void put_le32(uint8_t* p, uint32_t v) {
+  p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
+}
+
+// ChaChaKey::from_bytes (dpf.rs:277-316) into the device layout.
+int parse_key(const uint8_t* b, size_t len, KeyDev* k) {
+  if (!b) return fail(MG_EINVAL, "null key pointer");
+  if (len < 19 + 16) return fail(MG_EKEY, "invalid key format: byte array too short (%zu)", len);
+  const uint32_t d = b[18];
+  const size_t expected = 19 + (size_t)d * 18 + 16;
+  if (len != expected)
+    return fail(MG_EKEY, "invalid key format: invalid byte array length %zu (expected %zu)", len,
+                expected);
+  if (d > MG_MAX_DOMAIN_BITS)
+    return fail(MG_ERANGE, "key domain_bits %u exceeds the supported maximum %d", d,
+                MG_MAX_DOMAIN_BITS);
+  std::memset(k, 0, sizeof *k);
+  k->root_seed = make_uint4(le32(b), le32(b + 4), le32(b + 8), le32(b + 12));
+  k->root_t = b[16];
+  k->domain_bits = d;
+  size_t off = 19;
+  for (uint32_t l = 0; l < d; ++l) {
+    k->cw_seed[l] = make_uint4(le32(b + off), le32(b + off + 4), le32(b + off + 8), le32(b + off + 12));
+    k->cw_tl[l] = b[off + 16];
+    k->cw_tr[l] = b[off + 17];
+    off += 18;
+  }
+  k->final_cw = make_uint4(le32(b + off), le32(b + off + 4), le32(b + off + 8), le32(b + off + 12));
+  return MG_OK;
+}
+
+int wait_event(cudaEvent_t ev, uint32_t timeout_ms) {
+  if (timeout_ms == 0) {
+    MG_CUDA(cudaEventSynchronize(ev));
+    return MG_OK;
+  }
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) return MG_OK;
+    if (e != cudaErrorNotReady) return fail(MG_ECUDA, "cudaEventQuery: %s", cudaGetErrorString(e));
+    if (std::chrono::steady_clock::now() >= deadline)
+      return fail(MG_ETIMEDOUT, "pass not complete after %u ms", timeout_ms);
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+uint64_t domain_size(uint32_t d) { return 1ull << d; }
+
+}  // namespace
+
+struct mg_context {
+  int device = 0;
+  int sms = 0;
+  size_t smem_optin = 0;
+  std::mutex mu;              // serialises the one-call path (mg_scan)
+  std::mutex attr_mu;         // kernel attribute setup
+  size_t prepared_smem[9] = {0};
+  mg_batch* internal = nullptr;
+};
+
+struct mg_table {
+  mg_context* ctx = nullptr;
+  int device = 0;
+  int sms = 0;
+  void* d = nullptr;
+  uint64_t rows = 0;
+  uint32_t row_bytes = 0;
+};
+
+struct mg_batch {
+  struct Launch {
+    mg::ScanParams p;
+    uint32_t grid = 0;
+    size_t smem = 0;
+    int G = 1;
+    uint32_t col0 = 0;  // first share column of this launch
+  };
+  mg_context* ctx = nullptr;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr, ev_h0 = nullptr, ev_h1 = nullptr;
+  KeyDev* d_keys = nullptr;
+  KeyDev* h_keys = nullptr;
+  size_t cap_keys = 0;
+  uint4* d_partial = nullptr;
+  size_t cap_partial = 0;
+  uint4* d_out = nullptr;
+  uint8_t* h_out = nullptr;
+  size_t cap_out = 0;
+  std::vector<Launch> launches;
+  uint32_t total_cols = 0;
+  std::vector<uint32_t> key_col;    // first share column of input key i
+  std::vector<uint32_t> key_bytes;  // share bytes of input key i
+  size_t total_share_bytes = 0;
+  uint32_t shape_S = 0, shape_G = 0;
+  mg_plan_info info{};
+  bool planned = false;
+  bool launched = false;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<uint8_t> graph_sig;
+};
+
+namespace {
+
+template <class T>
+int set_device(const T* obj) {
+  MG_CUDA(cudaSetDevice(obj->device));
+  return MG_OK;
+}
+
+int prepare_g(mg_context* ctx, int G, size_t smem) {
+  std::lock_guard<std::mutex> lk(ctx->attr_mu);
+  if (ctx->prepared_smem[G] >= smem) return MG_OK;
+  MG_CUDA(mg::scan_prepare(G, smem));
+  ctx->prepared_smem[G] = smem;
+  return MG_OK;
+}
+
+int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4) {
+  if (nkeys > b->cap_keys) {
+    if (b->d_keys) cudaFree(b->d_keys);
+    if (b->h_keys) cudaFreeHost(b->h_keys);
+    b->d_keys = nullptr;
+    b->h_keys = nullptr;
+    b->cap_keys = 0;
+    if (cudaMalloc(&b->d_keys, nkeys * sizeof(KeyDev)) != cudaSuccess ||
+        cudaMallocHost(&b->h_keys, nkeys * sizeof(KeyDev)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MG_ENOMEM, "cannot allocate key buffers for %zu keys", nkeys);
+    }
+    b->cap_keys = nkeys;
+  }
+  if (partial_u4 > b->cap_partial) {
+    if (b->d_partial) cudaFree(b->d_partial);
+    b->d_partial = nullptr;
+    b->cap_partial = 0;
+    if (cudaMalloc(&b->d_partial, partial_u4 * 16) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MG_ENOMEM, "cannot allocate %zu-byte partial buffer", partial_u4 * 16);
+    }
+    b->cap_partial = partial_u4;
+  }
+  if (out_u4 > b->cap_out) {
+    if (b->d_out) cudaFree(b->d_out);
+    if (b->h_out) cudaFreeHost(b->h_out);
+    b->d_out = nullptr;
+    b->h_out = nullptr;
+    b->cap_out = 0;
+    if (cudaMalloc(&b->d_out, out_u4 * 16) != cudaSuccess ||
+        cudaMallocHost(&b->h_out, out_u4 * 16) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MG_ENOMEM, "cannot allocate share buffers (%zu bytes)", out_u4 * 16);
+    }
+    b->cap_out = out_u4;
+  }
+  return MG_OK;
+}
+
+struct SegPlan {
+  const mg_table* table;
+  uint32_t d;
+  std::vector<uint32_t> keys;  // input key indices, group-major
+  uint32_t g;
+};
+
+// Heuristic launch shape.  Keys per CTA: rows of up to 128 B leave the pass
+// bound by ChaCha8 issue slots, so one key per CTA maximises occupancy (row
+// re-reads of sibling CTAs hit L2); wider rows share each row load across up
+// to 4 keys.  Tile depth: the deepest in [8, 14] that still gives at least
+// four waves of work items.
+int choose_g(uint32_t V, size_t nkeys, uint32_t pinned) {
+  int g = pinned ? (int)pinned : (V <= 8 ? 1 : 4);
+  if ((size_t)g > nkeys) g = (int)nkeys;
+  if (g < 1) g = 1;
+  while (!mg::scan_g_supported(g)) --g;
+  return g;
+}
+
+void shape_for(uint32_t d, uint32_t S_target, uint32_t& S, uint32_t& U, uint32_t& M) {
+  S = std::min(S_target, d);
+  U = S >= 1 ? std::min<uint32_t>(8u, S - 1) : 0u;
+  M = S - U;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mg_last_error(void) { return g_err.c_str(); }
+
+int mg_context_create(int device, mg_context** out) {
+  if (!out) return fail(MG_EINVAL, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(MG_ENODEV, "no CUDA device available");
+  }
+  if (device < 0 || device >= n) return fail(MG_EINVAL, "device %d out of range (%d devices)", device, n);
+  MG_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  MG_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(MG_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a only", device,
+                prop.major, prop.minor);
+  MG_CUDA(cudaFree(nullptr));
+  mg_context* c = new mg_context();
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  *out = c;
+  return MG_OK;
+}
+
+int mg_context_destroy(mg_context* ctx) {
+  if (!ctx) return MG_OK;
+  if (ctx->internal) mg_batch_destroy(ctx->internal);
+  delete ctx;
+  return MG_OK;
+}
+
+int mg_device_info(mg_context* ctx, int* sm_count, uint64_t* free_bytes, uint64_t* total_bytes) {
+  if (!ctx) return fail(MG_EINVAL, "null context");
+  if (int rc = set_device(ctx)) return rc;
+  size_t f = 0, t = 0;
+  MG_CUDA(cudaMemGetInfo(&f, &t));
+  if (sm_count) *sm_count = ctx->sms;
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
+  return MG_OK;
+}
+
+// ---- tables -----------------------------------------------------------------
+
+int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table** out) {
+  if (!ctx || !out) return fail(MG_EINVAL, "null argument");
+  *out = nullptr;
+  if (row_bytes == 0 || row_bytes % 16 != 0 || row_bytes > MG_MAX_ROW_BYTES)
+    return fail(MG_EINVAL, "row_bytes %u must be a multiple of 16 in [16, %d]", row_bytes,
+                MG_MAX_ROW_BYTES);
+  if (rows > (1ull << MG_MAX_DOMAIN_BITS))
+    return fail(MG_ERANGE, "%llu rows exceed the 2^%d-row domain limit", (unsigned long long)rows,
+                MG_MAX_DOMAIN_BITS);
+  if (int rc = set_device(ctx)) return rc;
+  mg_table* t = new mg_table();
+  t->ctx = ctx;
+  t->device = ctx->device;
+  t->sms = ctx->sms;
+  t->rows = rows;
+  t->row_bytes = row_bytes;
+  const size_t bytes = (size_t)rows * row_bytes;
+  if (bytes) {
+    if (cudaMalloc(&t->d, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      delete t;
+      return fail(MG_ENOMEM, "cannot allocate a %zu-byte table", bytes);
+    }
+    if (cudaMemset(t->d, 0, bytes) != cudaSuccess) {
+      cudaFree(t->d);
+      delete t;
+      return fail(MG_ECUDA, "cudaMemset of the table failed");
+    }
+  }
+  *out = t;
+  return MG_OK;
+}
+
+int mg_table_destroy(mg_table* t) {
+  if (!t) return MG_OK;
+  set_device(t);
+  if (t->d) cudaFree(t->d);
+  delete t;
+  return MG_OK;
+}
+
+int mg_table_write_rows(mg_table* t, uint64_t first, const void* host, uint64_t n) {
+  if (!t || (!host && n)) return fail(MG_EINVAL, "null argument");
+  if (first > t->rows || n > t->rows - first)
+    return fail(MG_ERANGE, "rows [%llu, %llu) outside the %llu-row table", (unsigned long long)first,
+                (unsigned long long)(first + n), (unsigned long long)t->rows);
+  if (int rc = set_device(t)) return rc;
+  if (n) MG_CUDA(cudaMemcpy((uint8_t*)t->d + first * t->row_bytes, host, n * t->row_bytes,
+                            cudaMemcpyHostToDevice));
+  return MG_OK;
+}
+
+int mg_table_read_rows(const mg_table* t, uint64_t first, void* host, uint64_t n) {
+  if (!t || (!host && n)) return fail(MG_EINVAL, "null argument");
+  if (first > t->rows || n > t->rows - first)
+    return fail(MG_ERANGE, "rows [%llu, %llu) outside the %llu-row table", (unsigned long long)first,
+                (unsigned long long)(first + n), (unsigned long long)t->rows);
+  if (int rc = set_device(t)) return rc;
+  if (n) MG_CUDA(cudaMemcpy(host, (const uint8_t*)t->d + first * t->row_bytes, n * t->row_bytes,
+                            cudaMemcpyDeviceToHost));
+  return MG_OK;
+}
+
+int mg_table_fill_splitmix(mg_table* t, uint64_t seed) {
+  if (!t) return fail(MG_EINVAL, "null table");
+  if (int rc = set_device(t)) return rc;
+  MG_CUDA(mg::launch_fill_splitmix(t->d, t->rows * t->row_bytes / 8, seed, t->sms, nullptr));
+  MG_CUDA(cudaDeviceSynchronize());
+  return MG_OK;
+}
+
+int mg_table_xor_rows(mg_table* t, const uint64_t* idx, const void* diffs, uint64_t n) {
+  if (!t || (n && (!idx || !diffs))) return fail(MG_EINVAL, "null argument");
+  if (n == 0) return MG_OK;
+  for (uint64_t i = 0; i < n; ++i)
+    if (idx[i] >= t->rows)
+      return fail(MG_ERANGE, "row %llu outside the %llu-row table", (unsigned long long)idx[i],
+                  (unsigned long long)t->rows);
+  if (int rc = set_device(t)) return rc;
+  void* d_idx = nullptr;
+  void* d_diff = nullptr;
+  if (cudaMalloc(&d_idx, n * 8) != cudaSuccess || cudaMalloc(&d_diff, n * t->row_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (d_idx) cudaFree(d_idx);
+    return fail(MG_ENOMEM, "cannot stage %llu delta rows", (unsigned long long)n);
+  }
+  int rc = MG_OK;
+  cudaError_t e = cudaMemcpy(d_idx, idx, n * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_diff, diffs, n * t->row_bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = mg::launch_xor_rows(t->d, t->row_bytes / 16, (const uint64_t*)d_idx, d_diff, n,
+                                                t->sms, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) rc = fail(MG_ECUDA, "xor_rows: %s", cudaGetErrorString(e));
+  cudaFree(d_idx);
+  cudaFree(d_diff);
+  return rc;
+}
+
+uint64_t mg_table_rows(const mg_table* t) { return t ? t->rows : 0; }
+uint32_t mg_table_row_bytes(const mg_table* t) { return t ? t->row_bytes : 0; }
+const void* mg_table_device_ptr(const mg_table* t) { return t ? t->d : nullptr; }
+
+// ---- keys -------------------------------------------------------------------
+
+size_t mg_key_size(uint32_t d) { return 19 + (size_t)d * 18 + 16; }
+
+int mg_key_check(const uint8_t* key, size_t len, uint32_t* domain_bits, uint8_t* party) {
+  KeyDev k;
+  if (int rc = parse_key(key, len, &k)) return rc;
+  if (domain_bits) *domain_bits = k.domain_bits;
+  if (party) *party = key[17];
+  return MG_OK;
+}
+
+int mg_keygen(uint32_t d, uint64_t target, const uint8_t root0[16], const uint8_t root1[16],
+              uint8_t* key0, uint8_t* key1) {
+  if (!root0 || !root1 || !key0 || !key1) return fail(MG_EINVAL, "null argument");
+  if (d == 0 || d > 32) return fail(MG_EINVAL, "invalid domain bits %u: must be in [1, 32]", d);
+  if (target >= domain_size(d))
+    return fail(MG_ERANGE, "page index %llu exceeds max %llu", (unsigned long long)target,
+                (unsigned long long)domain_size(d));
+  uint32_t s0[4], s1[4];
+  for (int i = 0; i < 4; ++i) { s0[i] = le32(root0 + 4 * i); s1[i] = le32(root1 + 4 * i); }
+  uint8_t t0 = 0, t1 = 1;
+  const size_t len = mg_key_size(d);
+  for (int i = 0; i < 16; ++i) { key0[i] = root0[i]; key1[i] = root1[i]; }
+  key0[16] = 0; key1[16] = 1;
+  key0[17] = 0; key1[17] = 1;
+  key0[18] = (uint8_t)d; key1[18] = (uint8_t)d;
+  size_t off = 19;
+  for (uint32_t lvl = 0; lvl < d; ++lvl) {
+    uint32_t L0[4], R0[4], L1[4], R1[4];
+    uint8_t lt0, rt0, lt1, rt1;
+    host_expand(s0, L0, R0, lt0, rt0);
+    host_expand(s1, L1, R1, lt1, rt1);
+    const int bit = (int)((target >> (d - 1 - lvl)) & 1u);
+    const uint32_t* keep0 = bit ? R0 : L0;
+    const uint32_t* lose0 = bit ? L0 : R0;
+    const uint32_t* keep1 = bit ? R1 : L1;
+    const uint32_t* lose1 = bit ? L1 : R1;
+    const uint8_t keep_t0 = bit ? rt0 : lt0, lose_t0 = bit ? lt0 : rt0;
+    const uint8_t keep_t1 = bit ? rt1 : lt1, lose_t1 = bit ? lt1 : rt1;
+    uint32_t cw[4];
+    for (int i = 0; i < 4; ++i) cw[i] = lose0[i] ^ lose1[i];
+    const uint8_t tcw_lose = (uint8_t)(lose_t0 ^ lose_t1 ^ t0 ^ t1 ^ 1);
+    const uint8_t tcw_keep = (uint8_t)(keep_t0 ^ keep_t1 ^ t0 ^ t1);
+    for (int i = 0; i < 4; ++i) { put_le32(key0 + off + 4 * i, cw[i]); put_le32(key1 + off + 4 * i, cw[i]); }
+    key0[off + 16] = key1[off + 16] = bit ? tcw_lose : tcw_keep;
+    key0[off + 17] = key1[off + 17] = bit ? tcw_keep : tcw_lose;
+    off += 18;
+    for (int i = 0; i < 4; ++i) {
+      s0[i] = keep0[i] ^ (t0 == 1 ? cw[i] : 0u);
+      s1[i] = keep1[i] ^ (t1 == 1 ? cw[i] : 0u);
+    }
+    const uint8_t n0 = (uint8_t)(keep_t0 ^ (t0 == 1 ? tcw_keep : 0));
+    const uint8_t n1 = (uint8_t)(keep_t1 ^ (t1 == 1 ? tcw_keep : 0));
+    t0 = n0;
+    t1 = n1;
+  }
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t f = s0[i] ^ s1[i] ^ 0xFFFFFFFFu;
+    put_le32(key0 + off + 4 * i, f);
+    put_le32(key1 + off + 4 * i, f);
+  }
+  (void)len;
+  return MG_OK;
+}
+
+// ---- workspaces -------------------------------------------------------------
+
+int mg_batch_create(mg_context* ctx, mg_batch** out) {
+  if (!ctx || !out) return fail(MG_EINVAL, "null argument");
+  *out = nullptr;
+  if (int rc = set_device(ctx)) return rc;
+  mg_batch* b = new mg_batch();
+  b->ctx = ctx;
+  b->device = ctx->device;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev_k0) != cudaSuccess || cudaEventCreate(&b->ev_k1) != cudaSuccess ||
+      cudaEventCreate(&b->ev_h0) != cudaSuccess || cudaEventCreate(&b->ev_h1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    mg_batch_destroy(b);
+    return fail(MG_ECUDA, "cannot create workspace stream/events");
+  }
+  *out = b;
+  return MG_OK;
+}
+
+int mg_batch_destroy(mg_batch* b) {
+  if (!b) return MG_OK;
+  set_device(b);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->d_keys) cudaFree(b->d_keys);
+  if (b->h_keys) cudaFreeHost(b->h_keys);
+  if (b->d_partial) cudaFree(b->d_partial);
+  if (b->d_out) cudaFree(b->d_out);
+  if (b->h_out) cudaFreeHost(b->h_out);
+  for (cudaEvent_t e : {b->ev_k0, b->ev_k1, b->ev_done, b->ev_h0, b->ev_h1})
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return MG_OK;
+}
+
+int mg_batch_set_shape(mg_batch* b, uint32_t subtree_bits, uint32_t keys_per_cta) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (subtree_bits > 32) return fail(MG_EINVAL, "subtree_bits %u > 32", subtree_bits);
+  if (keys_per_cta && !mg::scan_g_supported((int)keys_per_cta))
+    return fail(MG_EINVAL, "keys_per_cta %u not in {1,2,3,4,8}", keys_per_cta);
+  b->shape_S = subtree_bits;
+  b->shape_G = keys_per_cta;
+  return MG_OK;
+}
+
+int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t* const* keys,
+                      const size_t* key_lens, uint32_t nkeys) {
+  if (!b || !tables || !keys || !key_lens) return fail(MG_EINVAL, "null argument");
+  if (nkeys == 0) return fail(MG_EINVAL, "no keys");
+  if (int rc = set_device(b)) return rc;
+  if (b->launched && cudaEventQuery(b->ev_done) == cudaErrorNotReady)
+    return fail(MG_EBUSY, "workspace still owns a pass in flight");
+  cudaGetLastError();
+  mg_context* ctx = b->ctx;
+
+  // Parse keys and group them into (table, domain) segments.
+  std::vector<KeyDev> parsed(nkeys);
+  std::vector<SegPlan> segs;
+  for (uint32_t i = 0; i < nkeys; ++i) {
+    const mg_table* t = tables[i];
+    if (!t) return fail(MG_EINVAL, "null table for key %u", i);
+    if (t->ctx != ctx) return fail(MG_EINVAL, "table of key %u belongs to another context", i);
+    if (int rc = parse_key(keys[i], key_lens[i], &parsed[i])) return rc;
+    const uint32_t d = parsed[i].domain_bits;
+    if (t->rows > domain_size(d))
+      return fail(MG_ERANGE, "more rows than domain size: %llu rows, key %u has %u domain bits",
+                  (unsigned long long)t->rows, i, d);
+    auto it = std::find_if(segs.begin(), segs.end(),
+                           [&](const SegPlan& s) { return s.table == t && s.d == d; });
+    if (it == segs.end()) {
+      segs.push_back(SegPlan{t, d, {}, 1});
+      it = segs.end() - 1;
+    }
+    it->keys.push_back(i);
+  }
+
+  // Keys per CTA from the widest-row segment with the most keys; split
+  // segments whose key count is not a multiple of it.
+  uint32_t Vmax = 1;
+  size_t nmax = 1;
+  for (const SegPlan& s : segs) {
+    Vmax = std::max(Vmax, s.table->row_bytes / 16);
+    nmax = std::max(nmax, s.keys.size());
+  }
+  const int G = choose_g(Vmax, nmax, b->shape_G);
+  std::vector<SegPlan> split;
+  for (SegPlan& s : segs) {
+    const uint32_t g = (uint32_t)std::min<size_t>((size_t)G, s.keys.size());
+    const size_t full = s.keys.size() / g * g;
+    SegPlan a{s.table, s.d, std::vector<uint32_t>(s.keys.begin(), s.keys.begin() + full), g};
+    split.push_back(a);
+    if (full < s.keys.size()) {
+      SegPlan r{s.table, s.d, std::vector<uint32_t>(s.keys.begin() + full, s.keys.end()),
+                (uint32_t)(s.keys.size() - full)};
+      split.push_back(r);
+    }
+  }
+
+  // Choose the tile depth: the deepest that still yields >= 4 waves.
+  const uint32_t S_candidates_hi = 14, S_candidates_lo = 8;
+  uint32_t S_target = b->shape_S ? b->shape_S : S_candidates_hi;
+  std::vector<mg_batch::Launch> launches;
+  uint32_t total_cols = 0;
+  std::vector<uint32_t> key_col(nkeys), key_bytes(nkeys), key_slot(nkeys);
+  size_t max_partial = 0;
+  for (;;) {
+    launches.clear();
+    total_cols = 0;
+    max_partial = 0;
+    uint64_t total_items = 0;
+    size_t key_cursor = 0;
+    for (size_t s0 = 0; s0 < split.size(); s0 += mg::kMaxSegs) {
+      mg_batch::Launch L;
+      std::memset(&L.p, 0, sizeof L.p);
+      L.G = G;
+      L.col0 = total_cols;
+      uint32_t slots = 2, cols = 0;
+      uint64_t items = 0;
+      const size_t s1 = std::min(split.size(), s0 + mg::kMaxSegs);
+      for (size_t si = s0; si < s1; ++si) {
+        const SegPlan& sp = split[si];
+        mg::Segment& sg = L.p.seg[si - s0];
+        uint32_t S, U, M;
+        shape_for(sp.d, S_target, S, U, M);
+        sg.table = reinterpret_cast<const uint4*>(sp.table->d);
+        sg.rows = sp.table->rows;
+        sg.V = sp.table->row_bytes / 16;
+        sg.d = sp.d;
+        sg.S = S;
+        sg.U = U;
+        sg.M = M;
+        sg.g = sp.g;
+        sg.groups = (uint32_t)(sp.keys.size() / sp.g);
+        sg.tiles = (uint32_t)((sp.table->rows + (1ull << S) - 1) >> S);
+        sg.item_begin = items;
+        sg.key_base = (uint32_t)key_cursor;
+        sg.col_base = cols;
+        for (size_t j = 0; j < sp.keys.size(); ++j) {
+          const uint32_t ki = sp.keys[j];
+          key_col[ki] = L.col0 + cols + (uint32_t)j * sg.V;
+          key_bytes[ki] = sp.table->row_bytes;
+          key_slot[ki] = (uint32_t)(key_cursor + j);
+        }
+        key_cursor += sp.keys.size();
+        items += (uint64_t)sg.tiles * sg.groups;
+        cols += (uint32_t)sp.keys.size() * sg.V;
+        slots = std::max(slots, M);
+      }
+      L.p.nsegs = (uint32_t)(s1 - s0);
+      L.p.items = items;
+      L.p.cols = cols;
+      L.p.slots = slots;
+      L.smem = mg::scan_smem_bytes(G, slots);
+      launches.push_back(L);
+      total_cols += cols;
+      total_items += items;
+    }
+    // Occupancy of the chosen shape.
+    bool ok = true;
+    uint64_t min_slots = UINT64_MAX;
+    for (mg_batch::Launch& L : launches) {
+      if (L.smem > ctx->smem_optin) { ok = false; break; }
+      if (int rc = prepare_g(ctx, G, L.smem)) return rc;
+      const int occ = mg::scan_occupancy(G, L.smem);
+      if (occ <= 0) { ok = false; break; }
+      const uint64_t slots_total = (uint64_t)occ * ctx->sms;
+      L.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(L.p.items, slots_total));
+      min_slots = std::min(min_slots, slots_total);
+      max_partial = std::max(max_partial, (size_t)L.grid * L.p.cols);
+    }
+    const bool enough = ok && total_items >= 4 * min_slots;
+    if (b->shape_S || enough || S_target <= S_candidates_lo) {
+      if (!ok) return fail(MG_EINVAL, "launch shape S=%u G=%d does not fit the device", S_target, G);
+      break;
+    }
+    --S_target;
+  }
+
+  if (int rc = grow(b, nkeys, max_partial, total_cols)) return rc;
+  for (uint32_t i = 0; i < nkeys; ++i) b->h_keys[key_slot[i]] = parsed[i];
+  for (mg_batch::Launch& L : launches) {
+    L.p.keys = b->d_keys;
+    L.p.partial = b->d_partial;
+  }
+  MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * sizeof(KeyDev),
+                          cudaMemcpyHostToDevice, b->stream));
+  b->launches = std::move(launches);
+  b->total_cols = total_cols;
+  b->key_col = std::move(key_col);
+  b->key_bytes = std::move(key_bytes);
+  b->total_share_bytes = 0;
+  for (uint32_t i = 0; i < nkeys; ++i) b->total_share_bytes += b->key_bytes[i];
+  b->info.subtree_bits = 0;
+  for (const mg_batch::Launch& L : b->launches)
+    for (uint32_t s = 0; s < L.p.nsegs; ++s) b->info.subtree_bits = std::max(b->info.subtree_bits, L.p.seg[s].S);
+  b->info.keys_per_cta = (uint32_t)G;
+  b->info.grid = b->launches[0].grid;
+  b->info.items = (uint32_t)b->launches[0].p.items;
+  b->info.segments = (uint32_t)split.size();
+  b->info.smem_bytes = (uint32_t)b->launches[0].smem;
+  b->planned = true;
+  return MG_OK;
+}
+
+static int enqueue_pass(mg_batch* b, cudaStream_t st) {
+  for (const mg_batch::Launch& L : b->launches) {
+    MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
+    MG_CUDA(mg::launch_reduce(b->d_partial, L.grid, L.p.cols, b->d_out + L.col0, st));
+  }
+  return MG_OK;
+}
+
+int mg_batch_launch(mg_batch* b, void* stream) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (!b->planned) return fail(MG_EINVAL, "mg_batch_set_keys has not been called");
+  if (int rc = set_device(b)) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  if (st != b->stream) {
+    // keys were staged on the workspace stream
+    MG_CUDA(cudaEventRecord(b->ev_done, b->stream));
+    MG_CUDA(cudaStreamWaitEvent(st, b->ev_done, 0));
+  }
+  MG_CUDA(cudaEventRecord(b->ev_k0, st));
+  if (int rc = enqueue_pass(b, st)) return rc;
+  MG_CUDA(cudaEventRecord(b->ev_k1, st));
+  MG_CUDA(cudaEventRecord(b->ev_done, st));
+  b->launched = true;
+  return MG_OK;
+}
+
+int mg_batch_launch_graph(mg_batch* b, void* stream) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (!b->planned) return fail(MG_EINVAL, "mg_batch_set_keys has not been called");
+  if (int rc = set_device(b)) return rc;
+  // Signature: everything baked into the captured kernel nodes.
+  std::vector<uint8_t> sig;
+  for (const mg_batch::Launch& L : b->launches) {
+    const uint8_t* pp = reinterpret_cast<const uint8_t*>(&L);
+    sig.insert(sig.end(), pp, pp + sizeof L);
+  }
+  const uint8_t* op = reinterpret_cast<const uint8_t*>(&b->d_out);
+  sig.insert(sig.end(), op, op + sizeof b->d_out);
+  if (!b->gexec || sig != b->graph_sig) {
+    if (b->gexec) {
+      cudaGraphExecDestroy(b->gexec);
+      b->gexec = nullptr;
+    }
+    cudaStream_t cap;
+    MG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int rc = MG_OK;
+    if (e == cudaSuccess) {
+      rc = enqueue_pass(b, cap);
+      e = cudaStreamEndCapture(cap, &graph);
+    }
+    if (e == cudaSuccess && rc == MG_OK) e = cudaGraphInstantiate(&b->gexec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap);
+    if (rc != MG_OK) return rc;
+    if (e != cudaSuccess) return fail(MG_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+    b->graph_sig = sig;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  if (st != b->stream) {
+    MG_CUDA(cudaEventRecord(b->ev_done, b->stream));
+    MG_CUDA(cudaStreamWaitEvent(st, b->ev_done, 0));
+  }
+  MG_CUDA(cudaEventRecord(b->ev_k0, st));
+  MG_CUDA(cudaGraphLaunch(b->gexec, st));
+  MG_CUDA(cudaEventRecord(b->ev_k1, st));
+  MG_CUDA(cudaEventRecord(b->ev_done, st));
+  b->launched = true;
+  return MG_OK;
+}
+
+int mg_batch_read(mg_batch* b, uint8_t* out, void* stream) {
+  if (!b || !out) return fail(MG_EINVAL, "null argument");
+  if (!b->launched) return fail(MG_EINVAL, "no pass launched");
+  if (int rc = set_device(b)) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  if (st != b->stream) {
+    MG_CUDA(cudaStreamWaitEvent(b->stream, b->ev_done, 0));
+  }
+  MG_CUDA(cudaEventRecord(b->ev_h0, b->stream));
+  MG_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, (size_t)b->total_cols * 16, cudaMemcpyDeviceToHost,
+                          b->stream));
+  MG_CUDA(cudaEventRecord(b->ev_h1, b->stream));
+  MG_CUDA(cudaEventRecord(b->ev_done, b->stream));
+  MG_CUDA(cudaEventSynchronize(b->ev_done));
+  size_t off = 0;
+  for (size_t i = 0; i < b->key_col.size(); ++i) {
+    std::memcpy(out + off, b->h_out + (size_t)b->key_col[i] * 16, b->key_bytes[i]);
+    off += b->key_bytes[i];
+  }
+  return MG_OK;
+}
+
+int mg_batch_sync(mg_batch* b, uint32_t timeout_ms) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (!b->launched) return MG_OK;
+  if (int rc = set_device(b)) return rc;
+  return wait_event(b->ev_done, timeout_ms);
+}
+
+int mg_batch_shares_device(mg_batch* b, const void** dptr, size_t* bytes) {
+  if (!b || !dptr) return fail(MG_EINVAL, "null argument");
+  *dptr = b->d_out;
+  if (bytes) *bytes = (size_t)b->total_cols * 16;
+  return MG_OK;
+}
+
+int mg_batch_plan(mg_batch* b, mg_plan_info* info) {
+  if (!b || !info) return fail(MG_EINVAL, "null argument");
+  if (!b->planned) return fail(MG_EINVAL, "mg_batch_set_keys has not been called");
+  *info = b->info;
+  return MG_OK;
+}
+
+int mg_batch_last_kernel_ns(mg_batch* b, uint64_t* ns) {
+  if (!b || !ns) return fail(MG_EINVAL, "null argument");
+  if (!b->launched) return fail(MG_EINVAL, "no pass launched");
+  if (int rc = set_device(b)) return rc;
+  float ms = 0.f;
+  MG_CUDA(cudaEventSynchronize(b->ev_k1));
+  MG_CUDA(cudaEventElapsedTime(&ms, b->ev_k0, b->ev_k1));
+  *ns = (uint64_t)((double)ms * 1e6);
+  return MG_OK;
+}
+
+// ---- one-call scan ----------------------------------------------------------
+
+int mg_scan(mg_context* ctx, const mg_table* const* tables, const uint8_t* const* keys,
+            const size_t* key_lens, uint32_t nkeys, uint8_t* out, uint32_t timeout_ms,
+            mg_timing* timing) {
+  if (!ctx || !out) return fail(MG_EINVAL, "null argument");
+  const auto t0 = std::chrono::steady_clock::now();
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (int rc = set_device(ctx)) return rc;
+  if (!ctx->internal) {
+    mg_batch* b = nullptr;
+    if (int rc = mg_batch_create(ctx, &b)) return rc;
+    ctx->internal = b;
+  }
+  mg_batch* b = ctx->internal;
+  if (b->launched && cudaEventQuery(b->ev_done) == cudaErrorNotReady)
+    return fail(MG_EBUSY, "the previous pass on this context has not completed");
+  cudaGetLastError();
+  int rc = mg_batch_set_keys(b, tables, keys, key_lens, nkeys);
+  if (rc) return rc;
+  MG_CUDA(cudaEventRecord(b->ev_h0, b->stream));  // key H2D was enqueued before this point
+  if ((rc = mg_batch_launch(b, nullptr))) return rc;
+  MG_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, (size_t)b->total_cols * 16, cudaMemcpyDeviceToHost,
+                          b->stream));
+  MG_CUDA(cudaEventRecord(b->ev_h1, b->stream));
+  MG_CUDA(cudaEventRecord(b->ev_done, b->stream));
+  if ((rc = wait_event(b->ev_done, timeout_ms))) return rc;
+  size_t off = 0;
+  for (size_t i = 0; i < b->key_col.size(); ++i) {
+    std::memcpy(out + off, b->h_out + (size_t)b->key_col[i] * 16, b->key_bytes[i]);
+    off += b->key_bytes[i];
+  }
+  if (timing) {
+    float k_ms = 0.f, d_ms = 0.f;
+    cudaEventElapsedTime(&k_ms, b->ev_k0, b->ev_k1);
+    cudaEventElapsedTime(&d_ms, b->ev_k1, b->ev_h1);
+    timing->kernel_ns = (uint64_t)((double)k_ms * 1e6);
+    timing->d2h_ns = (uint64_t)((double)d_ms * 1e6);
+    timing->total_ns = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                           std::chrono::steady_clock::now() - t0).count();
+    const uint64_t rest = timing->kernel_ns + timing->d2h_ns;
+    timing->h2d_ns = timing->total_ns > rest ? timing->total_ns - rest : 0;
+  }
+  return MG_OK;
+}
+
+// ---- point evaluation -------------------------------------------------------
+
+int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const uint64_t* idx, uint64_t n,
+                   uint8_t* out) {
+  if (!ctx || (n && (!idx || !out))) return fail(MG_EINVAL, "null argument");
+  KeyDev k;
+  if (int rc = parse_key(key, key_len, &k)) return rc;
+  if (n == 0) return MG_OK;
+  if (int rc = set_device(ctx)) return rc;
+  void *d_key = nullptr, *d_idx = nullptr, *d_out = nullptr;
+  if (cudaMalloc(&d_key, sizeof k) != cudaSuccess || cudaMalloc(&d_idx, n * 8) != cudaSuccess ||
+      cudaMalloc(&d_out, n * 16) != cudaSuccess) {
+    cudaGetLastError();
+    if (d_key) cudaFree(d_key);
+    if (d_idx) cudaFree(d_idx);
+    return fail(MG_ENOMEM, "cannot stage %llu evaluation points", (unsigned long long)n);
+  }
+  cudaError_t e = cudaMemcpy(d_key, &k, sizeof k, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_idx, idx, n * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = mg::launch_eval_points((const KeyDev*)d_key, (const uint64_t*)d_idx, n, d_out, ctx->sms, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, n * 16, cudaMemcpyDeviceToHost);
+  cudaFree(d_key);
+  cudaFree(d_idx);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(MG_ECUDA, "eval_points: %s", cudaGetErrorString(e));
+  return MG_OK;
+}
+
+}  // extern "C"

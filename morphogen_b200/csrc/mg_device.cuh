@@ -1,0 +1,147 @@
+// mg_device.cuh -- device-side ChaCha8 GGM PRG and DPF key layout (sm_100a).
+//
+// The PRG is the reference's ChaCha8Prg::expand
+// (crates/morphogen-gpu-dpf/src/chacha_prg.rs:153-178): ChaCha key = seed||seed,
+// nonce 0, two blocks with counters 0 and 1 (RFC 8439 state layout, 4 double
+// rounds, feed-forward add, chacha_prg.rs:112-144).  Children: L = block0[0..4],
+// R = block0[4..8], tL = block1[0] & 1, tR = block1[1] & 1.
+//
+// B200 notes: the path is integer-ALU bound.  Adds and 3-input logic run at
+// the full 128 lanes/clk/SM, funnel shifts and byte permutes at half rate, so
+// the code is issue-bound at ~12 instructions per quarter round.  Both blocks
+// are written out in one straight-line function so the compiler shares the
+// three counter-independent column quarter rounds of round 1 and drops the
+// parts of block 1 that do not reach bit 0 of words 0 and 1.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mg {
+
+constexpr int kThreads = 256;    // CTA size of the scan kernel
+constexpr int kMaxLevels = 32;   // MG_MAX_DOMAIN_BITS
+constexpr int kMaxSegs = 8;      // (table, domain) segments per launch
+constexpr uint32_t kSigma0 = 0x61707865u;  // "expand 32-byte k"
+constexpr uint32_t kSigma1 = 0x3320646eu;
+constexpr uint32_t kSigma2 = 0x79622d32u;
+constexpr uint32_t kSigma3 = 0x6b206574u;
+
+// Device key: the wire key (dpf.rs:259-274) re-laid out for 16-byte loads.
+// t bytes keep the reference's byte semantics (a node applies its correction
+// word iff t == 1, dpf.rs:122,192,228).
+struct alignas(16) KeyDev {
+  uint4 root_seed;
+  uint4 final_cw;
+  uint4 cw_seed[kMaxLevels];
+  uint8_t cw_tl[kMaxLevels];
+  uint8_t cw_tr[kMaxLevels];
+  uint32_t root_t;
+  uint32_t domain_bits;
+  uint32_t pad[2];
+};
+static_assert(sizeof(KeyDev) == 624, "KeyDev layout");
+
+__device__ __forceinline__ uint32_t rotl16(uint32_t x) { return __byte_perm(x, 0, 0x1032); }
+__device__ __forceinline__ uint32_t rotl8(uint32_t x) { return __byte_perm(x, 0, 0x2103); }
+__device__ __forceinline__ uint32_t rotl12(uint32_t x) { return __funnelshift_l(x, x, 12); }
+__device__ __forceinline__ uint32_t rotl7(uint32_t x) { return __funnelshift_l(x, x, 7); }
+
+#define MG_QR(a, b, c, d)              \
+  a += b; d ^= a; d = mg::rotl16(d);   \
+  c += d; b ^= c; b = mg::rotl12(b);   \
+  a += b; d ^= a; d = mg::rotl8(d);    \
+  c += d; b ^= c; b = mg::rotl7(b);
+
+#define MG_DOUBLE_ROUND(x)                                        \
+  MG_QR(x##0, x##4, x##8, x##12) MG_QR(x##1, x##5, x##9, x##13)   \
+  MG_QR(x##2, x##6, x##10, x##14) MG_QR(x##3, x##7, x##11, x##15) \
+  MG_QR(x##0, x##5, x##10, x##15) MG_QR(x##1, x##6, x##11, x##12) \
+  MG_QR(x##2, x##7, x##8, x##13) MG_QR(x##3, x##4, x##9, x##14)
+
+// ChaCha8Prg::expand.  tl/tr are 0 or 1.
+__device__ __forceinline__ void prg_expand(const uint4 s, uint4& L, uint4& R, uint32_t& tl,
+                                           uint32_t& tr) {
+  uint32_t x0 = kSigma0, x1 = kSigma1, x2 = kSigma2, x3 = kSigma3;
+  uint32_t x4 = s.x, x5 = s.y, x6 = s.z, x7 = s.w;
+  uint32_t x8 = s.x, x9 = s.y, x10 = s.z, x11 = s.w;
+  uint32_t x12 = 0u, x13 = 0u, x14 = 0u, x15 = 0u;
+  uint32_t y0 = kSigma0, y1 = kSigma1, y2 = kSigma2, y3 = kSigma3;
+  uint32_t y4 = s.x, y5 = s.y, y6 = s.z, y7 = s.w;
+  uint32_t y8 = s.x, y9 = s.y, y10 = s.z, y11 = s.w;
+  uint32_t y12 = 1u, y13 = 0u, y14 = 0u, y15 = 0u;
+  MG_DOUBLE_ROUND(x) MG_DOUBLE_ROUND(y)
+  MG_DOUBLE_ROUND(x) MG_DOUBLE_ROUND(y)
+  MG_DOUBLE_ROUND(x) MG_DOUBLE_ROUND(y)
+  MG_DOUBLE_ROUND(x) MG_DOUBLE_ROUND(y)
+  L = make_uint4(x0 + kSigma0, x1 + kSigma1, x2 + kSigma2, x3 + kSigma3);
+  R = make_uint4(x4 + s.x, x5 + s.y, x6 + s.z, x7 + s.w);
+  tl = (y0 + kSigma0) & 1u;
+  tr = (y1 + kSigma1) & 1u;
+  (void)x8; (void)x9; (void)x10; (void)x11; (void)x12; (void)x13; (void)x14; (void)x15;
+  (void)y2; (void)y3; (void)y4; (void)y5; (void)y6; (void)y7; (void)y8; (void)y9;
+  (void)y10; (void)y11; (void)y12; (void)y13; (void)y14; (void)y15;
+}
+
+// One GGM node expansion with the level's correction word applied to both
+// children when t == 1 (dpf.rs:221-239).
+__device__ __forceinline__ void expand_cw(const uint4 s, const uint32_t t, const KeyDev& k,
+                                          const uint32_t level, uint4& L, uint32_t& tl, uint4& R,
+                                          uint32_t& tr) {
+  const uint4 cw = k.cw_seed[level];
+  const uint32_t cwl = k.cw_tl[level];
+  const uint32_t cwr = k.cw_tr[level];
+  prg_expand(s, L, R, tl, tr);
+  const uint32_t m = (t == 1u) ? 0xFFFFFFFFu : 0u;
+  L.x ^= cw.x & m; L.y ^= cw.y & m; L.z ^= cw.z & m; L.w ^= cw.w & m;
+  R.x ^= cw.x & m; R.y ^= cw.y & m; R.z ^= cw.z & m; R.w ^= cw.w & m;
+  tl ^= cwl & m;
+  tr ^= cwr & m;
+}
+
+// Leaf output: seed, XOR final_cw when t == 1 (dpf.rs:136-139, 211-218).
+__device__ __forceinline__ uint4 leaf_mask(const uint4 s, const uint32_t t, const KeyDev& k) {
+  const uint32_t m = (t == 1u) ? 0xFFFFFFFFu : 0u;
+  const uint4 f = k.final_cw;
+  return make_uint4(s.x ^ (f.x & m), s.y ^ (f.y & m), s.z ^ (f.z & m), s.w ^ (f.w & m));
+}
+
+__device__ __forceinline__ uint4 xor_and(uint4 acc, const uint4 d, const uint4 m) {
+  acc.x ^= d.x & m.x; acc.y ^= d.y & m.y; acc.z ^= d.z & m.z; acc.w ^= d.w & m.w;
+  return acc;
+}
+__device__ __forceinline__ uint4 xor4(uint4 a, const uint4 b) {
+  a.x ^= b.x; a.y ^= b.y; a.z ^= b.z; a.w ^= b.w;
+  return a;
+}
+
+// One (table, domain) segment of a pass.  Work items of the segment are
+// (tile, group) pairs, tile-major so that CTAs running at the same time
+// share row tiles through L2.
+struct Segment {
+  const uint4* table;   // rows * V uint4, row-major
+  uint64_t rows;        // rows scanned (<= 2^d)
+  uint64_t item_begin;  // first global item index of the segment
+  uint32_t tiles;       // ceil(rows / 2^S)
+  uint32_t groups;      // key groups
+  uint32_t V;           // uint4 per row (row_bytes / 16), 1..256
+  uint32_t d;           // domain bits of every key in the segment
+  uint32_t S;           // tile depth: 2^S leaves per item (S <= d)
+  uint32_t U;           // breadth-first levels below the tile root (2^U DFS roots)
+  uint32_t M;           // depth-first levels per thread (S - U)
+  uint32_t g;           // keys per group (<= kernel G)
+  uint32_t key_base;    // KeyDev index of group 0, key 0
+  uint32_t col_base;    // partial column of group 0, key 0, lane 0
+};
+
+struct ScanParams {
+  Segment seg[kMaxSegs];
+  const KeyDev* keys;
+  uint4* partial;       // [gridDim.x][cols]
+  uint64_t items;
+  uint32_t nsegs;
+  uint32_t cols;        // total share uint4s of the pass
+  uint32_t slots;       // stack slots per key per thread allocated in smem
+};
+
+}  // namespace mg

@@ -1,0 +1,25 @@
+// mg_internal.h -- launchers shared between the kernels and the C ABI layer.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mg_device.cuh"
+
+namespace mg {
+
+size_t scan_smem_bytes(int G, uint32_t slots);
+bool scan_g_supported(int G);
+cudaError_t scan_prepare(int G, size_t smem);
+int scan_occupancy(int G, size_t smem);
+cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st);
+cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
+                          cudaStream_t st);
+cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, int sms, cudaStream_t st);
+cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const void* diffs,
+                            uint64_t n, int sms, cudaStream_t st);
+cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
+                               cudaStream_t st);
+
+}  // namespace mg

@@ -1,0 +1,379 @@
+// mg_kernels.cu -- sm_100a kernels of the per-server PIR answer path.
+//
+// scan_kernel<G>: persistent CTAs walk a list of (tile, key group) work items.
+// For one item (an aligned subtree of 2^S rows and g <= G keys):
+//   1. threads 0..g-1 walk each key from its root to the tile root (d - S
+//      levels; the prefix walk of dpf.rs:183-203);
+//   2. the CTA expands U levels breadth-first in shared memory, giving every
+//      thread one node 2^M leaves above the rows (the GGM tree of
+//      dpf.rs:210-246 in breadth-first order);
+//   3. each thread walks its node depth-first with a per-thread stack in
+//      shared memory, one leaf pair per step; the 16-byte leaf outputs
+//      (masks) of all g keys go to shared memory;
+//   4. the CTA scans the step's rows with coalesced 128-bit loads and
+//      XOR-accumulates row & mask per key in registers (kernel.rs:1243-1256);
+//   5. after the last step the per-thread accumulators are XOR-reduced with
+//      warp shuffles and shared memory and folded into this CTA's own row of
+//      the partial buffer (no atomics).
+// reduce_kernel XORs the per-CTA partial rows into the shares.  XOR is
+// associative and commutative, so the shares are bit-exact whatever the
+// schedule.  The kernels contain no waits on other CTAs or on the host.
+#include "mg_device.cuh"
+#include "mg_internal.h"
+
+namespace mg {
+
+template <int G>
+__global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ ScanParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  KeyDev* s_keys = reinterpret_cast<KeyDev*>(smem_raw);
+  uint4* s_mask = reinterpret_cast<uint4*>(smem_raw + G * sizeof(KeyDev));  // [G][2*T]
+  uint4* s_seed = s_mask + G * 2 * kThreads;                                 // [G][slots][T]
+  uint8_t* s_t = reinterpret_cast<uint8_t*>(s_seed + (size_t)G * p.slots * kThreads);
+  const uint32_t tid = threadIdx.x;
+  const uint32_t slots = p.slots;
+
+  uint4* my_partial = p.partial + (size_t)blockIdx.x * p.cols;
+  for (uint32_t c = tid; c < p.cols; c += kThreads) my_partial[c] = make_uint4(0u, 0u, 0u, 0u);
+
+  for (uint64_t item = blockIdx.x; item < p.items; item += gridDim.x) {
+    uint32_t si = 0;
+    while (si + 1 < p.nsegs && item >= p.seg[si + 1].item_begin) ++si;
+    const Segment& sg = p.seg[si];
+    const uint64_t local = item - sg.item_begin;
+    const uint32_t tile = (uint32_t)(local / sg.groups);
+    const uint32_t group = (uint32_t)(local % sg.groups);
+    const uint32_t g = sg.g, V = sg.V, d = sg.d, S = sg.S, U = sg.U, M = sg.M;
+    const uint32_t L0 = d - S;
+
+    __syncthreads();  // the previous item is done with shared memory
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(p.keys + sg.key_base + (size_t)group * g);
+      uint4* dst = reinterpret_cast<uint4*>(s_keys);
+      const uint32_t n = g * (uint32_t)(sizeof(KeyDev) / 16);
+      for (uint32_t i = tid; i < n; i += kThreads) dst[i] = src[i];
+    }
+    __syncthreads();
+
+    // 1. prefix walk to the tile root; the breadth-first ping-pong below
+    //    starts in slot (U & 1) so that it ends in slot 0.
+    const uint32_t start_slot = U & 1u;
+    if (tid < g) {
+      const KeyDev& K = s_keys[tid];
+      uint4 s = K.root_seed;
+      uint32_t t = K.root_t;
+      for (uint32_t lvl = 0; lvl < L0; ++lvl) {
+        uint4 Lc, Rc;
+        uint32_t tl, tr;
+        expand_cw(s, t, K, lvl, Lc, tl, Rc, tr);
+        const uint32_t bit = (tile >> (L0 - 1 - lvl)) & 1u;
+        s = bit ? Rc : Lc;
+        t = bit ? tr : tl;
+      }
+      s_seed[(tid * slots + start_slot) * kThreads] = s;
+      s_t[(tid * slots + start_slot) * kThreads] = (uint8_t)t;
+    }
+    __syncthreads();
+
+    // 2. breadth-first expansion of U levels below the tile root.
+    uint32_t cur = start_slot;
+    for (uint32_t j = 0; j < U; ++j) {
+      const uint32_t nxt = cur ^ 1u;
+      const uint32_t work = g << j;
+      for (uint32_t it = tid; it < work; it += kThreads) {
+        const uint32_t k = it >> j, i = it & ((1u << j) - 1u);
+        const size_t src = (k * slots + cur) * kThreads + i;
+        const size_t dst = (k * slots + nxt) * kThreads + 2 * i;
+        uint4 Lc, Rc;
+        uint32_t tl, tr;
+        expand_cw(s_seed[src], s_t[src], s_keys[k], L0 + j, Lc, tl, Rc, tr);
+        s_seed[dst] = Lc;
+        s_seed[dst + 1] = Rc;
+        s_t[dst] = (uint8_t)tl;
+        s_t[dst + 1] = (uint8_t)tr;
+      }
+      __syncthreads();
+      cur = nxt;
+    }
+
+    // 3-4. depth-first leaf pairs + scan of the step's rows.
+    uint4 acc[G];
+#pragma unroll
+    for (int k = 0; k < G; ++k) acc[k] = make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t NR = 1u << U;
+    const uint32_t pairs = M ? (1u << (M - 1)) : 1u;
+    const uint64_t tile_row0 = (uint64_t)tile << S;
+    const uint32_t rpi = kThreads / V;  // rows per scan sweep
+    const uint32_t lane = tid % V, rslot = tid / V;
+    const bool scan_thread = tid < rpi * V;
+    const uint4* __restrict__ tbl = sg.table;
+    const uint64_t nrows = sg.rows;
+    const uint32_t abs0 = d - M;  // tree level of the depth-first roots
+
+    for (uint32_t pi = 0; pi < pairs; ++pi) {
+      if (tid < NR) {
+#pragma unroll 1
+        for (uint32_t k = 0; k < g; ++k) {
+          const KeyDev& K = s_keys[k];
+          uint4* col_seed = s_seed + (size_t)k * slots * kThreads + tid;
+          uint8_t* col_t = s_t + (size_t)k * slots * kThreads + tid;
+          uint4* mk = s_mask + (size_t)k * 2 * kThreads + 2 * tid;
+          if (M == 0) {
+            mk[0] = leaf_mask(col_seed[0], col_t[0], K);
+            mk[1] = make_uint4(0u, 0u, 0u, 0u);
+            continue;
+          }
+          // Pair pi's parent path re-joins the stack at relative level
+          // M - 1 - ctz(pi) (root for pi == 0).
+          uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
+          uint4 s = col_seed[lvl * kThreads];
+          uint32_t t = col_t[lvl * kThreads];
+          for (;; ++lvl) {
+            uint4 Lc, Rc;
+            uint32_t tl, tr;
+            expand_cw(s, t, K, abs0 + lvl, Lc, tl, Rc, tr);
+            if (lvl == M - 1) {
+              mk[0] = leaf_mask(Lc, tl, K);
+              mk[1] = leaf_mask(Rc, tr, K);
+              break;
+            }
+            col_seed[(lvl + 1) * kThreads] = Rc;
+            col_t[(lvl + 1) * kThreads] = (uint8_t)tr;
+            s = Lc;
+            t = tl;
+          }
+        }
+      }
+      __syncthreads();
+      if (scan_thread) {
+        for (uint32_t r = rslot; r < 2 * NR; r += rpi) {
+          const uint64_t row = tile_row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
+          if (row < nrows) {
+            const uint4 dat = __ldg(tbl + row * V + lane);
+#pragma unroll
+            for (int k = 0; k < G; ++k)
+              if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat, s_mask[(size_t)k * 2 * kThreads + r]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // 5. reduce the accumulators of threads holding the same lane.
+    uint4* s_red = s_mask;  // G * T uint4 fit in the mask buffer
+    const bool pow2 = (V & (V - 1)) == 0;
+    if (pow2 && V < 32) {
+#pragma unroll
+      for (int k = 0; k < G; ++k) {
+        uint4 v = acc[k];
+        for (uint32_t off = 16; off >= V; off >>= 1) {
+          v.x ^= __shfl_xor_sync(0xFFFFFFFFu, v.x, off);
+          v.y ^= __shfl_xor_sync(0xFFFFFFFFu, v.y, off);
+          v.z ^= __shfl_xor_sync(0xFFFFFFFFu, v.z, off);
+          v.w ^= __shfl_xor_sync(0xFFFFFFFFu, v.w, off);
+        }
+        if ((tid & 31u) < V) s_red[(size_t)k * kThreads + (tid >> 5) * V + (tid & 31u)] = v;
+      }
+      __syncthreads();
+      for (uint32_t o = tid; o < g * V; o += kThreads) {
+        const uint32_t k = o / V, ln = o % V;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        for (uint32_t w = 0; w < kThreads / 32; ++w) v = xor4(v, s_red[(size_t)k * kThreads + w * V + ln]);
+        const size_t col = sg.col_base + ((size_t)group * g + k) * V + ln;
+        my_partial[col] = xor4(my_partial[col], v);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < G; ++k)
+        s_red[(size_t)k * kThreads + tid] = scan_thread ? acc[k] : make_uint4(0u, 0u, 0u, 0u);
+      __syncthreads();
+      for (uint32_t o = tid; o < g * V; o += kThreads) {
+        const uint32_t k = o / V, ln = o % V;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        for (uint32_t j = 0; j < rpi; ++j) v = xor4(v, s_red[(size_t)k * kThreads + ln + j * V]);
+        const size_t col = sg.col_base + ((size_t)group * g + k) * V + ln;
+        my_partial[col] = xor4(my_partial[col], v);
+      }
+    }
+  }
+}
+
+// out[c] = XOR over the nparts per-CTA partial rows.  Block = cpb columns x
+// (kThreads / cpb) slices; the slices are combined in shared memory.
+__global__ void __launch_bounds__(kThreads) reduce_kernel(const uint4* __restrict__ partial,
+                                                          uint32_t nparts, uint32_t cols,
+                                                          uint4* __restrict__ out) {
+  __shared__ uint4 red[kThreads];
+  const uint32_t cpb = cols < 32u ? cols : 32u;
+  const uint32_t slices = kThreads / cpb;
+  const uint32_t cl = threadIdx.x % cpb, sl = threadIdx.x / cpb;
+  const uint32_t c = blockIdx.x * cpb + cl;
+  uint4 v = make_uint4(0u, 0u, 0u, 0u);
+  if (c < cols && sl < slices)
+    for (uint32_t j = sl; j < nparts; j += slices) v = xor4(v, partial[(size_t)j * cols + c]);
+  red[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < cpb && c < cols) {
+    uint4 r = make_uint4(0u, 0u, 0u, 0u);
+    for (uint32_t s = 0; s < slices; ++s) r = xor4(r, red[s * cpb + threadIdx.x]);
+    out[c] = r;
+  }
+}
+
+// SplitMix64 output `w` of the stream seeded with `seed` (Steele, Lea, Flood 2014).
+__device__ __forceinline__ uint64_t splitmix_word(uint64_t seed, uint64_t w) {
+  uint64_t z = seed + (w + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fill_splitmix_kernel(uint2* __restrict__ dst, uint64_t words, uint64_t seed) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
+    const uint64_t z = splitmix_word(seed, w);
+    dst[w] = make_uint2((uint32_t)z, (uint32_t)(z >> 32));
+  }
+}
+
+// table[row_idx[e]] ^= diff[e]; XOR atomics make duplicate rows in one batch
+// order-independent.
+__global__ void xor_rows_kernel(uint4* __restrict__ table, uint32_t V, const uint64_t* __restrict__ idx,
+                                const uint4* __restrict__ diffs, uint64_t n) {
+  const uint64_t total = n * V;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const uint64_t e = i / V;
+    const uint32_t ln = (uint32_t)(i % V);
+    const uint4 dv = diffs[i];
+    unsigned int* t = reinterpret_cast<unsigned int*>(table + idx[e] * V + ln);
+    atomicXor(t + 0, dv.x);
+    atomicXor(t + 1, dv.y);
+    atomicXor(t + 2, dv.z);
+    atomicXor(t + 3, dv.w);
+  }
+}
+
+// ChaChaKey::eval (dpf.rs:103-142) at n indices, one thread per index.
+__global__ void eval_points_kernel(const KeyDev* __restrict__ key, const uint64_t* __restrict__ idx,
+                                   uint64_t n, uint4* __restrict__ out) {
+  __shared__ KeyDev sk;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(key);
+    uint4* dst = reinterpret_cast<uint4*>(&sk);
+    for (uint32_t i = threadIdx.x; i < sizeof(KeyDev) / 16; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t x = idx[i];
+    uint4 s = sk.root_seed;
+    uint32_t t = sk.root_t;
+    const uint32_t d = sk.domain_bits;
+    for (uint32_t lvl = 0; lvl < d; ++lvl) {
+      uint4 Lc, Rc;
+      uint32_t tl, tr;
+      expand_cw(s, t, sk, lvl, Lc, tl, Rc, tr);
+      const uint32_t bit = (uint32_t)(x >> (d - 1 - lvl)) & 1u;
+      s = bit ? Rc : Lc;
+      t = bit ? tr : tl;
+    }
+    out[i] = leaf_mask(s, t, sk);
+  }
+}
+
+// ---- host-side launchers --------------------------------------------------
+
+size_t scan_smem_bytes(int G, uint32_t slots) {
+  return (size_t)G * (sizeof(KeyDev) + 2 * kThreads * 16 + (size_t)slots * kThreads * 17);
+}
+
+template <int G>
+static cudaError_t launch_scan_t(const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st) {
+  scan_kernel<G><<<grid, kThreads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int G>
+static cudaError_t prepare_t(size_t smem) {
+  return cudaFuncSetAttribute(scan_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <int G>
+static int occupancy_t(size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_kernel<G>, kThreads, smem) != cudaSuccess)
+    return 0;
+  return n;
+}
+
+#define MG_G_DISPATCH(G_, EXPR1, EXPR2, EXPR3, EXPR4, EXPR8) \
+  switch (G_) {                                              \
+    case 1: return EXPR1;                                    \
+    case 2: return EXPR2;                                    \
+    case 3: return EXPR3;                                    \
+    case 4: return EXPR4;                                    \
+    case 8: return EXPR8;                                    \
+    default: break;                                          \
+  }
+
+bool scan_g_supported(int G) { return G == 1 || G == 2 || G == 3 || G == 4 || G == 8; }
+
+cudaError_t scan_prepare(int G, size_t smem) {
+  MG_G_DISPATCH(G, prepare_t<1>(smem), prepare_t<2>(smem), prepare_t<3>(smem), prepare_t<4>(smem),
+                prepare_t<8>(smem));
+  return cudaErrorInvalidValue;
+}
+
+int scan_occupancy(int G, size_t smem) {
+  MG_G_DISPATCH(G, occupancy_t<1>(smem), occupancy_t<2>(smem), occupancy_t<3>(smem),
+                occupancy_t<4>(smem), occupancy_t<8>(smem));
+  return 0;
+}
+
+cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st) {
+  MG_G_DISPATCH(G, launch_scan_t<1>(p, grid, smem, st), launch_scan_t<2>(p, grid, smem, st),
+                launch_scan_t<3>(p, grid, smem, st), launch_scan_t<4>(p, grid, smem, st),
+                launch_scan_t<8>(p, grid, smem, st));
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
+                          cudaStream_t st) {
+  const uint32_t cpb = cols < 32u ? cols : 32u;
+  if (cols == 0) return cudaSuccess;
+  reduce_kernel<<<(cols + cpb - 1) / cpb, kThreads, 0, st>>>(partial, nparts, cols, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, int sms, cudaStream_t st) {
+  if (words == 0) return cudaSuccess;
+  uint64_t blocks = (words + 255) / 256;
+  const uint64_t cap = (uint64_t)sms * 16;
+  if (blocks > cap) blocks = cap;
+  fill_splitmix_kernel<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<uint2*>(dst), words, seed);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const void* diffs,
+                            uint64_t n, int sms, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  uint64_t blocks = (n * V + 255) / 256;
+  const uint64_t cap = (uint64_t)sms * 16;
+  if (blocks > cap) blocks = cap;
+  xor_rows_kernel<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<uint4*>(table), V, idx,
+                                                     reinterpret_cast<const uint4*>(diffs), n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
+                               cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  uint64_t blocks = (n + 127) / 128;
+  const uint64_t cap = (uint64_t)sms * 8;
+  if (blocks > cap) blocks = cap;
+  eval_points_kernel<<<(unsigned)blocks, 128, 0, st>>>(key, idx, n, reinterpret_cast<uint4*>(out));
+  return cudaGetLastError();
+}
+
+}  // namespace mg
