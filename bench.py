@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the per-server PIR answer path on B200.
+
+Default workload (one step = one scan pass answering one query):
+  plain single query at mainnet scale -- a table of 2^31 rows x 32 B (64 GiB)
+  of SplitMix64 bytes from seed 0, 3 ChaCha8 DPF keys (one server's shares)
+  over a 31-bit domain for 3 uniformly drawn target rows.
+
+`value` is scanned GB/s (table bytes per pass / device time per pass, keys
+resident); `e2e` is the same metric through the one-call C entry point
+mg_scan with host keys in and host shares out.  The roofline object reports
+the dominant kernel (the fused subtree-expansion + scan kernel) against the
+measured HBM copy bandwidth, and `alu` reports it against the ChaCha8 PRG
+ceiling measured in the same run (the binding resource on this workload).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload plain31|plain20|batched31 --queries Q]
+
+Multi-GPU (torchrun, one process per GPU): every rank serves an independent
+replica of the table (replicas only; the path needs no collective), timing is
+the max over ranks and `value` the aggregate over all replicas.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "plain31": dict(name="plain single query, 2^31 rows x 32 B (64 GiB), 31-bit keys",
+                    rows=1 << 31, row_bytes=32, d=31),
+    "plain20": dict(name="plain single query, 2^20 rows x 256 B (256 MiB), 20-bit keys",
+                    rows=1 << 20, row_bytes=256, d=20),
+    "batched31": dict(name="batched queries per pass, 2^31 rows x 32 B (64 GiB), 31-bit keys",
+                      rows=1 << 31, row_bytes=32, d=31),
+}
+KEYS_PER_QUERY = 3
+SEED = 0
+CPU_SAMPLE_ROWS = 1 << 28      # aligned window timed on the host cores (cpu_baseline)
+REF_SAMPLE_ROWS = 1 << 25      # per-step sample of the reference arm
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def seeded_keys(d: int, rows: int, nqueries: int, seed: int = SEED):
+    """Targets uniform in [0, rows), root seeds from a seeded generator;
+    returns (party-0 keys, party-1 keys, targets)."""
+    from morphogen_b200 import gpu_dpf as G
+    rng = np.random.default_rng(seed)
+    targets = [int(t) for t in rng.integers(0, rows, nqueries * KEYS_PER_QUERY)]
+    k0, k1 = [], []
+    p = G.ChaChaParams(d)
+    for t in targets:
+        a, b = G.generate_chacha_dpf_keys(p, t, rng)
+        k0.append(a)
+        k1.append(b)
+    return k0, k1, targets
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def cpu_scan_sample(keys, rows_total: int, row_bytes: int, sample_rows: int, reps: int = 1):
+    """Time the oracle (the restated reference CPU scan: eval_fused_3dpf_cpu
+    with scalar ChaCha8, OpenMP over all host threads) on an aligned window of
+    the table.  Returns (GB/s per rep list, threads, description)."""
+    import oracle
+    oracle.build()
+    base = (rows_total // 2) // sample_rows * sample_rows
+    host = oracle.fill_splitmix(base * row_bytes, sample_rows * row_bytes, SEED)
+    kb = [bytes(k) for k in keys]
+    nthreads = os.cpu_count() or 1
+    rates = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        oracle.scan_fused(kb, host, row_bytes, row_base=base, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        rates.append(sample_rows * row_bytes / dt / 1e9)
+    desc = (f"{len(kb)} keys over the aligned window of {sample_rows} rows starting at row {base} "
+            f"({sample_rows * row_bytes / 2**30:.1f} GiB); GB/s of that window")
+    return rates, nthreads, desc
+
+
+def run_reference(args, rank: int, world: int):
+    """The reference's CPU implementation of the path (oracle port) on the host cores."""
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    nq = args.queries if args.workload == "batched31" else 1
+    k0, _, _ = seeded_keys(wl["d"], wl["rows"], nq)
+    sample = min(REF_SAMPLE_ROWS, wl["rows"])
+    _, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.warmup)
+    rates, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.steps)
+    v = sum(rates) / len(rates)
+    gb_pass = wl["rows"] * wl["row_bytes"] / 1e9
+    line = {
+        "impl": "reference", "metric": "scanned GB/s", "value": round(v, 4), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(gb_pass / v * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nq * KEYS_PER_QUERY,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": desc + "; ms_per_step extrapolates to the full table"},
+        "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank: int, world: int, local_rank: int):
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local_rank)
+
+    wl = WORKLOADS[args.workload]
+    nq = args.queries if args.workload == "batched31" else 1
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    scanner = G.GpuScanner(local_rank)
+    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
+    k0, k1, targets = seeded_keys(d, rows, nq)
+    nkeys = len(k0)
+
+    # Correctness gate (outside timing): both servers' shares XOR to the targets.
+    ws = scanner.workspace()
+    ws.set_keys([table] * nkeys, k1)
+    ws.launch()
+    s1 = ws.read()
+    ws.set_keys([table] * nkeys, k0)
+    ws.launch()
+    s0 = ws.read()
+    verified = all(bytes(a ^ b for a, b in zip(x, y)) == table.read_rows(t, 1).tobytes()
+                   for x, y, t in zip(s0, s1, targets))
+    if not verified:
+        raise SystemExit("bench: shares do not reconstruct the target rows")
+    plan = ws.plan()
+
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    for _ in range(args.warmup):
+        ws.launch(stream=sh)
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    scan_ns = []
+    clocks = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        ws.launch(stream=sh)
+        ev[i][1].record(stream)
+        scan_ns.append(ws.last_scan_ns())  # waits for this pass; device time of the scan kernel
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    bytes_pass = rows * rb
+    value = world * bytes_pass / (ms_per_step * 1e-3) / 1e9
+
+    # e2e: host keys in, host shares out, through mg_scan.
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        shares, _ = scanner.scan_keys(table, k0)
+        dt = (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            e2e_ms.append(dt)
+    assert shares == s0
+    e2e_per = sum(e2e_ms) / len(e2e_ms)
+    if dist:
+        tt = torch.tensor([e2e_per], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_per = float(tt.item())
+    e2e_value = world * bytes_pass / (e2e_per * 1e-3) / 1e9
+
+    # Rooflines of the dominant kernel.
+    peaks = measured_peaks()
+    scan_avg_s = sum(scan_ns) / len(scan_ns) * 1e-9
+    achieved_hbm = bytes_pass / scan_avg_s / 1e9
+    hbm_peak = float(peaks["hbm_gbs"])
+    nodes = nkeys * ((1 << d) - 1)
+    prg_peak = scanner.prg_peak()
+    achieved_nodes = nodes / scan_avg_s
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        rates, threads, desc = cpu_scan_sample(k0, rows, rb, min(CPU_SAMPLE_ROWS, rows))
+        cpu = {"value": round(rates[0], 4), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": desc}
+
+    pct = lambda xs, q: float(np.percentile(np.array(xs), q))  # noqa: E731
+    line = {
+        "metric": "scanned GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nkeys,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "plan": plan, "l2": "inputs larger than L2 (64 GiB table)" if bytes_pass > 126e6
+                   else "table fits L2"},
+        "latency_ms": {"p50": round(pct(step_ms, 50), 3), "p99": round(pct(step_ms, 99), 3),
+                       "e2e_p50": round(pct(e2e_ms, 50), 3), "e2e_p99": round(pct(e2e_ms, 99), 3)},
+        "queries_per_s": round(world * nq / (ms_per_step * 1e-3), 3),
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
+                "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
+        "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved_hbm / hbm_peak, 4), "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                     if "fallback" not in peaks else "fallback 6650 GB/s"},
+        "alu": {"bound": "int32 issue (ChaCha8)", "achieved": round(achieved_nodes / 1e9, 3),
+                "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
+                "frac": round(achieved_nodes / prg_peak, 4),
+                "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "verified": verified,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mg", choices=["mg", "reference"])
+    ap.add_argument("--workload", default="plain31", choices=sorted(WORKLOADS))
+    ap.add_argument("--queries", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "mg":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

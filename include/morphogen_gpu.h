@@ -143,8 +143,15 @@ int mg_batch_read(mg_batch* batch, uint8_t* out_shares, void* stream);
 int mg_batch_sync(mg_batch* batch, uint32_t timeout_ms);
 int mg_batch_shares_device(mg_batch* batch, const void** dptr, size_t* bytes);
 int mg_batch_plan(mg_batch* batch, mg_plan_info* info);
-/* Timing of the last completed launch on the workspace stream. */
+/* Timing of the last launch on the workspace stream: scan + reduction
+ * kernels, and the scan kernels alone (a graph replay is timed as a whole). */
 int mg_batch_last_kernel_ns(mg_batch* batch, uint64_t* ns);
+int mg_batch_last_scan_ns(mg_batch* batch, uint64_t* ns);
+
+/* ---- measurement (no counterpart in the reference) ------------------------ */
+/* ChaCha8 node expansions per second of the device PRG alone (no memory
+ * traffic, full occupancy): the integer-ALU ceiling of the scan kernel. */
+int mg_prg_peak(mg_context* ctx, uint32_t iters, double* expands_per_s);
 
 /* ---- point evaluation on the device: ChaChaKey::eval (dpf.rs:103-142) ----- */
 /* out: n * 16 bytes, out[i] = eval(idx[i]).  Host arrays. */

@@ -33,7 +33,8 @@ EXPORTED = (
     "mg_table_device_ptr", "mg_key_size", "mg_key_check", "mg_keygen", "mg_scan",
     "mg_batch_create", "mg_batch_destroy", "mg_batch_set_keys", "mg_batch_set_shape",
     "mg_batch_launch", "mg_batch_launch_graph", "mg_batch_read", "mg_batch_sync",
-    "mg_batch_shares_device", "mg_batch_plan", "mg_batch_last_kernel_ns", "mg_eval_points",
+    "mg_batch_shares_device", "mg_batch_plan", "mg_batch_last_kernel_ns", "mg_batch_last_scan_ns",
+    "mg_eval_points", "mg_prg_peak",
 )
 
 
@@ -117,6 +118,8 @@ def lib():
             "mg_batch_shares_device": ([vp, C.POINTER(vp), C.POINTER(sz)], C.c_int),
             "mg_batch_plan": ([vp, C.POINTER(PlanInfo)], C.c_int),
             "mg_batch_last_kernel_ns": ([vp, u64p], C.c_int),
+            "mg_batch_last_scan_ns": ([vp, u64p], C.c_int),
+            "mg_prg_peak": ([vp, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
             "mg_eval_points": ([vp, u8p, sz, u64p, C.c_uint64, u8p], C.c_int),
         }
         for name, (args, res) in sig.items():

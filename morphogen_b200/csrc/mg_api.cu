@@ -156,7 +156,7 @@ struct mg_batch {
   mg_context* ctx = nullptr;
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr, ev_h0 = nullptr, ev_h1 = nullptr;
+  cudaEvent_t ev_k0 = nullptr, ev_km = nullptr, ev_k1 = nullptr, ev_done = nullptr, ev_h0 = nullptr, ev_h1 = nullptr;
   KeyDev* d_keys = nullptr;
   KeyDev* h_keys = nullptr;
   size_t cap_keys = 0;
@@ -488,7 +488,8 @@ int mg_batch_create(mg_context* ctx, mg_batch** out) {
   b->ctx = ctx;
   b->device = ctx->device;
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&b->ev_k0) != cudaSuccess || cudaEventCreate(&b->ev_k1) != cudaSuccess ||
+      cudaEventCreate(&b->ev_k0) != cudaSuccess || cudaEventCreate(&b->ev_km) != cudaSuccess ||
+      cudaEventCreate(&b->ev_k1) != cudaSuccess ||
       cudaEventCreate(&b->ev_h0) != cudaSuccess || cudaEventCreate(&b->ev_h1) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
@@ -509,7 +510,7 @@ int mg_batch_destroy(mg_batch* b) {
   if (b->d_partial) cudaFree(b->d_partial);
   if (b->d_out) cudaFree(b->d_out);
   if (b->h_out) cudaFreeHost(b->h_out);
-  for (cudaEvent_t e : {b->ev_k0, b->ev_k1, b->ev_done, b->ev_h0, b->ev_h1})
+  for (cudaEvent_t e : {b->ev_k0, b->ev_km, b->ev_k1, b->ev_done, b->ev_h0, b->ev_h1})
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -685,9 +686,13 @@ int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t*
   return MG_OK;
 }
 
-static int enqueue_pass(mg_batch* b, cudaStream_t st) {
-  for (const mg_batch::Launch& L : b->launches) {
+// mark: event recorded after the last scan launch (before its reduction),
+// so that the scan kernels can be timed apart from the reductions.
+static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
+  for (size_t i = 0; i < b->launches.size(); ++i) {
+    const mg_batch::Launch& L = b->launches[i];
     MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
+    if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
     MG_CUDA(mg::launch_reduce(b->d_partial, L.grid, L.p.cols, b->d_out + L.col0, st));
   }
   return MG_OK;
@@ -704,7 +709,7 @@ int mg_batch_launch(mg_batch* b, void* stream) {
     MG_CUDA(cudaStreamWaitEvent(st, b->ev_done, 0));
   }
   MG_CUDA(cudaEventRecord(b->ev_k0, st));
-  if (int rc = enqueue_pass(b, st)) return rc;
+  if (int rc = enqueue_pass(b, st, b->ev_km)) return rc;
   MG_CUDA(cudaEventRecord(b->ev_k1, st));
   MG_CUDA(cudaEventRecord(b->ev_done, st));
   b->launched = true;
@@ -734,7 +739,7 @@ int mg_batch_launch_graph(mg_batch* b, void* stream) {
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     int rc = MG_OK;
     if (e == cudaSuccess) {
-      rc = enqueue_pass(b, cap);
+      rc = enqueue_pass(b, cap, nullptr);
       e = cudaStreamEndCapture(cap, &graph);
     }
     if (e == cudaSuccess && rc == MG_OK) e = cudaGraphInstantiate(&b->gexec, graph, 0);
@@ -751,6 +756,7 @@ int mg_batch_launch_graph(mg_batch* b, void* stream) {
   }
   MG_CUDA(cudaEventRecord(b->ev_k0, st));
   MG_CUDA(cudaGraphLaunch(b->gexec, st));
+  MG_CUDA(cudaEventRecord(b->ev_km, st));  // a replayed pass is timed as a whole
   MG_CUDA(cudaEventRecord(b->ev_k1, st));
   MG_CUDA(cudaEventRecord(b->ev_done, st));
   b->launched = true;
@@ -808,6 +814,49 @@ int mg_batch_last_kernel_ns(mg_batch* b, uint64_t* ns) {
   MG_CUDA(cudaEventSynchronize(b->ev_k1));
   MG_CUDA(cudaEventElapsedTime(&ms, b->ev_k0, b->ev_k1));
   *ns = (uint64_t)((double)ms * 1e6);
+  return MG_OK;
+}
+
+int mg_batch_last_scan_ns(mg_batch* b, uint64_t* ns) {
+  if (!b || !ns) return fail(MG_EINVAL, "null argument");
+  if (!b->launched) return fail(MG_EINVAL, "no pass launched");
+  if (int rc = set_device(b)) return rc;
+  float ms = 0.f;
+  MG_CUDA(cudaEventSynchronize(b->ev_km));
+  MG_CUDA(cudaEventElapsedTime(&ms, b->ev_k0, b->ev_km));
+  *ns = (uint64_t)((double)ms * 1e6);
+  return MG_OK;
+}
+
+int mg_prg_peak(mg_context* ctx, uint32_t iters, double* expands_per_s) {
+  if (!ctx || !expands_per_s) return fail(MG_EINVAL, "null argument");
+  if (int rc = set_device(ctx)) return rc;
+  uint32_t blocks = 0, threads = 0;
+  uint32_t* d_out = nullptr;
+  MG_CUDA(mg::prg_peak_shape(ctx->sms, &blocks, &threads));
+  if (cudaMalloc(&d_out, (size_t)blocks * threads * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MG_ENOMEM, "cannot allocate the microbenchmark output");
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaError_t e = mg::launch_prg_peak(d_out, iters, blocks, threads, nullptr);  // warm-up
+  float best = 0.f;
+  for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+    cudaEventRecord(e0);
+    e = mg::launch_prg_peak(d_out, iters, blocks, threads, nullptr);
+    cudaEventRecord(e1);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && (best == 0.f || ms < best)) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(MG_ECUDA, "prg peak: %s", cudaGetErrorString(e));
+  *expands_per_s = (double)blocks * threads * iters / ((double)best * 1e-3);
   return MG_OK;
 }
 

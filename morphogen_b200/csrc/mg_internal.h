@@ -22,4 +22,8 @@ cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const 
 cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
                                cudaStream_t st);
 
+cudaError_t prg_peak_shape(int sms, uint32_t* blocks, uint32_t* threads);
+cudaError_t launch_prg_peak(uint32_t* out, uint32_t iters, uint32_t blocks, uint32_t threads,
+                            cudaStream_t st);
+
 }  // namespace mg

@@ -282,7 +282,39 @@ __global__ void eval_points_kernel(const KeyDev* __restrict__ key, const uint64_
   }
 }
 
+// PRG-only ceiling: every thread chains `iters` node expansions (left child,
+// t folded in) with no memory traffic -- the best the ChaCha8 code above can
+// do on this GPU, the ALU roofline of the scan kernel.
+__global__ void __launch_bounds__(256) prg_peak_kernel(uint32_t* __restrict__ out, uint32_t iters) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  uint4 s = make_uint4(tid, tid * 0x9E3779B9u, ~tid, 0x01234567u);
+  uint32_t acc = 0;
+  for (uint32_t i = 0; i < iters; ++i) {
+    uint4 L, R;
+    uint32_t tl, tr;
+    prg_expand(s, L, R, tl, tr);
+    s = make_uint4(L.x ^ R.w, L.y ^ tl, L.z ^ tr, L.w ^ R.x);
+    acc += R.y;
+  }
+  out[tid] = s.x ^ s.y ^ s.z ^ s.w ^ acc;
+}
+
 // ---- host-side launchers --------------------------------------------------
+
+cudaError_t prg_peak_shape(int sms, uint32_t* blocks, uint32_t* threads) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, prg_peak_kernel, 256, 0);
+  if (e != cudaSuccess) return e;
+  *threads = 256;
+  *blocks = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms * 4;
+  return cudaSuccess;
+}
+
+cudaError_t launch_prg_peak(uint32_t* out, uint32_t iters, uint32_t blocks, uint32_t threads,
+                            cudaStream_t st) {
+  prg_peak_kernel<<<blocks, threads, 0, st>>>(out, iters);
+  return cudaGetLastError();
+}
 
 size_t scan_smem_bytes(int G, uint32_t slots) {
   return (size_t)G * (sizeof(KeyDev) + 2 * kThreads * 16 + (size_t)slots * kThreads * 17);

@@ -381,6 +381,11 @@ class Workspace:
         N.check(N.lib().mg_batch_last_kernel_ns(self.handle, C.byref(v)))
         return v.value
 
+    def last_scan_ns(self) -> int:
+        v = C.c_uint64()
+        N.check(N.lib().mg_batch_last_scan_ns(self.handle, C.byref(v)))
+        return v.value
+
     def shares_device(self) -> tuple[int, int]:
         p = C.c_void_p()
         n = C.c_size_t()
@@ -421,6 +426,12 @@ class GpuScanner:
         total = C.c_uint64()
         N.check(N.lib().mg_device_info(self._ctx.handle, C.byref(sms), C.byref(free), C.byref(total)))
         return {"sm_count": sms.value, "free_bytes": free.value, "total_bytes": total.value}
+
+    def prg_peak(self, iters: int = 256) -> float:
+        """Node expansions/s of the device ChaCha8 PRG alone (ALU ceiling)."""
+        v = C.c_double()
+        N.check(N.lib().mg_prg_peak(self._ctx.handle, iters, C.byref(v)))
+        return v.value
 
     def workspace(self) -> Workspace:
         return Workspace(self)

@@ -347,9 +347,10 @@ uint64_t mgo_splitmix_word(uint64_t seed, uint64_t i) {
 }
 
 void mgo_fill_splitmix(uint8_t* buf, uint64_t off, uint64_t n, uint64_t seed) {
-  uint64_t o;
-  for (o = 0; o < n; o++) {
-    uint64_t g = off + o;
+  int64_t o;
+#pragma omp parallel for schedule(static)
+  for (o = 0; o < (int64_t)n; o++) {
+    uint64_t g = off + (uint64_t)o;
     buf[o] = (uint8_t)(mgo_splitmix_word(seed, g >> 3) >> (8 * (g & 7)));
   }
 }
