@@ -158,6 +158,38 @@ int mg_prg_peak(mg_context* ctx, uint32_t iters, double* expands_per_s);
 int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const uint64_t* idx,
                    uint64_t n, uint8_t* out);
 
+/* ---- allocation-free scan (no counterpart in the reference) -------------- */
+/* For callers that cannot call cudaMalloc: the host application or a memory
+ * pool owns all device memory (plugins, embedded servers), or cudaMalloc /
+ * cudaFree would block on or synchronise the device inside a latency-bound
+ * serving loop.  Same result as mg_scan for the same table and keys, but no
+ * device or pinned memory is allocated: the parsed keys and the per-CTA
+ * partial rows live in one fixed device array of MG_NOALLOC_SCRATCH_BYTES,
+ * which every GPU that loads the library holds until the process exits.
+ *
+ * table_dev: rows x row_bytes in device memory on `device`; out_shares_dev:
+ * nkeys * row_bytes of device memory, share i at offset i * row_bytes.  Keys
+ * are host bytes in the wire format and must all have the same domain_bits.
+ * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default)
+ * and the shares are valid once the stream reaches it.
+ *
+ * Limits: nkeys <= MG_NOALLOC_MAX_KEYS, and nkeys * 624 bytes of keys plus
+ * (persistent CTAs) x nkeys x row_bytes bytes of partial rows must fit the
+ * array; otherwise MG_ERANGE with a message naming the limit.  On B200
+ * (at most 592 CTAs) that is nkeys * row_bytes up to about 28 KB.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and enables the kernel's shared memory; make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: each call clears what it needs, but calls that overlap on the GPU
+ * (other streams, or host threads without ordering between them) race and
+ * must be serialised by the caller. */
+#define MG_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define MG_NOALLOC_MAX_KEYS 64
+int mg_scan_noalloc(int device, const void* table_dev, uint64_t rows, uint32_t row_bytes,
+                    const uint8_t* const* keys, const size_t* key_lens, uint32_t nkeys,
+                    void* out_shares_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

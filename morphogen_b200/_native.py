@@ -34,7 +34,7 @@ EXPORTED = (
     "mg_batch_create", "mg_batch_destroy", "mg_batch_set_keys", "mg_batch_set_shape",
     "mg_batch_launch", "mg_batch_launch_graph", "mg_batch_read", "mg_batch_sync",
     "mg_batch_shares_device", "mg_batch_plan", "mg_batch_last_kernel_ns", "mg_batch_last_scan_ns",
-    "mg_eval_points", "mg_prg_peak",
+    "mg_eval_points", "mg_prg_peak", "mg_scan_noalloc",
 )
 
 
@@ -121,6 +121,8 @@ def lib():
             "mg_batch_last_scan_ns": ([vp, u64p], C.c_int),
             "mg_prg_peak": ([vp, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
             "mg_eval_points": ([vp, u8p, sz, u64p, C.c_uint64, u8p], C.c_int),
+            "mg_scan_noalloc": ([C.c_int, vp, C.c_uint64, C.c_uint32, C.POINTER(u8p), C.POINTER(sz),
+                                 C.c_uint32, vp, vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -126,6 +126,10 @@ uint64_t domain_size(uint32_t d) { return 1ull << d; }
 
 }  // namespace
 
+namespace mg {
+void set_last_error(const char* msg) { g_err = msg ? msg : ""; }
+}  // namespace mg
+
 struct mg_context {
   int device = 0;
   int sms = 0;

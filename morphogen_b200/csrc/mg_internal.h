@@ -22,6 +22,9 @@ cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const 
 cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
                                cudaStream_t st);
 
+// Sets the thread-local message returned by mg_last_error().
+void set_last_error(const char* msg);
+
 cudaError_t prg_peak_shape(int sms, uint32_t* blocks, uint32_t* threads);
 cudaError_t launch_prg_peak(uint32_t* out, uint32_t iters, uint32_t blocks, uint32_t threads,
                             cudaStream_t st);
