@@ -40,6 +40,8 @@ sys.path.insert(0, str(ROOT))
 WORKLOADS = {
     "plain31": dict(name="plain single query, 2^31 rows x 32 B (64 GiB), 31-bit keys",
                     rows=1 << 31, row_bytes=32, d=31),
+    "plain31s": dict(name="profiling case: 2^25 rows x 32 B (1 GiB) scanned with 31-bit keys",
+                     rows=1 << 25, row_bytes=32, d=31),
     "plain20": dict(name="plain single query, 2^20 rows x 256 B (256 MiB), 20-bit keys",
                     rows=1 << 20, row_bytes=256, d=20),
     "batched31": dict(name="batched queries per pass, 2^31 rows x 32 B (64 GiB), 31-bit keys",
@@ -198,6 +200,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     # Correctness gate (outside timing): both servers' shares XOR to the targets.
     ws = scanner.workspace()
+    ws.set_kernel(args.kernel)
     ws.set_keys([table] * nkeys, k1)
     ws.launch()
     s1 = ws.read()
@@ -208,7 +211,20 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                    for x, y, t in zip(s0, s1, targets))
     if not verified:
         raise SystemExit("bench: shares do not reconstruct the target rows")
+    tuned = None
+    budget = args.autotune
+    if budget < 0:
+        ws.launch()
+        ws.sync()
+        budget = 5000 if ws.last_kernel_ns() < 20e6 and args.kernel == "auto" else 0
+    if budget > 0:
+        tuned = ws.autotune(budget)
+        ws.launch()
+        if ws.read() != s0:
+            raise SystemExit("bench: autotuned shape changed the shares")
     plan = ws.plan()
+    if tuned:
+        plan["autotuned_ms"] = round(tuned["ms"], 4)
 
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
@@ -306,7 +322,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                 "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
                 "frac": round(achieved_nodes / prg_peak, 4),
                 "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run"},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": plan["kernels"] * args.steps,
         "clocks": clk,
         "verified": verified,
     }
@@ -324,6 +340,10 @@ def main():
     ap.add_argument("--workload", default="plain31", choices=sorted(WORKLOADS))
     ap.add_argument("--queries", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--autotune", type=int, default=-1,
+                    help="autotuner budget in ms before timing (-1: 5000 when a pass is under 20 ms, else off)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "cta", "warp"],
+                    help="scan kernel for the device-resident passes (default: the planner's choice)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mg":
         args.warmup = 3

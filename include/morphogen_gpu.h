@@ -63,14 +63,23 @@ typedef struct {
   uint64_t total_ns;
 } mg_timing;
 
-/* Launch shape chosen for a pass (the autotuner's decision). */
+/* Scan kernels.  CTA: a CTA expands a 2^S-row tile (breadth-first in shared
+ * memory, then one depth-first walk per thread); any row size.  WARP: a
+ * frontier of tree nodes is computed breadth-first up front and every warp
+ * walks 32 x 2^M rows on its own; rows of 16..512 B (power of two). */
+enum { MG_KERNEL_AUTO = 0, MG_KERNEL_CTA = 1, MG_KERNEL_WARP = 2 };
+
+/* Launch shape chosen for a pass (first launch; subtree_bits over all). */
 typedef struct {
-  uint32_t subtree_bits;  /* leaves per work item = 2^subtree_bits (largest segment) */
-  uint32_t keys_per_cta;  /* keys evaluated together on one row tile */
-  uint32_t grid;          /* persistent CTAs launched */
-  uint32_t items;         /* (tile, key group) work items */
-  uint32_t segments;      /* (table, domain) segments in the pass */
-  uint32_t smem_bytes;    /* dynamic shared memory per CTA */
+  uint32_t subtree_bits;   /* rows per work item = 2^subtree_bits (CTA: S; warp: M + 5) */
+  uint32_t keys_per_cta;   /* keys evaluated together on one work item */
+  uint32_t grid;           /* persistent CTAs launched */
+  uint32_t items;          /* (tile, key group) work items */
+  uint32_t segments;       /* (table, domain) segments in the pass */
+  uint32_t smem_bytes;     /* dynamic shared memory per CTA */
+  uint32_t kernel;         /* MG_KERNEL_CTA or MG_KERNEL_WARP */
+  uint32_t frontier_nodes; /* frontier nodes held for the warp kernel */
+  uint32_t kernels;        /* kernel launches per pass (frontier chain, scans, reductions) */
 } mg_plan_info;
 
 /* ---- context: GpuScanner::new (kernel.rs:258-465) ------------------------ */
@@ -129,8 +138,17 @@ int mg_batch_destroy(mg_batch* batch);
  * workspace stream.  Reallocates device buffers only when they grow. */
 int mg_batch_set_keys(mg_batch* batch, const mg_table* const* tables, const uint8_t* const* keys,
                       const size_t* key_lens, uint32_t nkeys);
-/* Pin the launch shape (0 = let the autotuner choose). */
+/* Pin the launch shape (0 = let the planner choose). */
 int mg_batch_set_shape(mg_batch* batch, uint32_t subtree_bits, uint32_t keys_per_cta);
+/* Choose the scan kernel (MG_KERNEL_AUTO by default). */
+int mg_batch_set_kernel(mg_batch* batch, int kind);
+/* Autotuner: with keys set, time candidate launch shapes (both kernels, work
+ * item depth, keys per item) on the device for up to budget_ms (0 = all),
+ * check that every shape gives identical shares, keep the fastest for this
+ * workload (rows, row size, depth, key count of every segment) in the
+ * context -- later passes with the same signature use it unless a shape is
+ * pinned -- and re-plan this workspace with it.  best/best_ms may be NULL. */
+int mg_batch_autotune(mg_batch* batch, uint32_t budget_ms, mg_plan_info* best, double* best_ms);
 /* Enqueue the scan and reduction kernels on `stream` (a cudaStream_t; NULL =
  * the workspace's own stream).  Keys and tables must already be resident.
  * Launch-only: capturable into a CUDA graph by the caller. */

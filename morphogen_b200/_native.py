@@ -31,7 +31,8 @@ EXPORTED = (
     "mg_table_create", "mg_table_destroy", "mg_table_write_rows", "mg_table_read_rows",
     "mg_table_fill_splitmix", "mg_table_xor_rows", "mg_table_rows", "mg_table_row_bytes",
     "mg_table_device_ptr", "mg_key_size", "mg_key_check", "mg_keygen", "mg_scan",
-    "mg_batch_create", "mg_batch_destroy", "mg_batch_set_keys", "mg_batch_set_shape",
+    "mg_batch_create", "mg_batch_destroy", "mg_batch_set_keys", "mg_batch_set_shape", "mg_batch_set_kernel",
+    "mg_batch_autotune",
     "mg_batch_launch", "mg_batch_launch_graph", "mg_batch_read", "mg_batch_sync",
     "mg_batch_shares_device", "mg_batch_plan", "mg_batch_last_kernel_ns", "mg_batch_last_scan_ns",
     "mg_eval_points", "mg_prg_peak", "mg_scan_noalloc",
@@ -66,7 +67,11 @@ class Timing(C.Structure):
 
 class PlanInfo(C.Structure):
     _fields_ = [("subtree_bits", C.c_uint32), ("keys_per_cta", C.c_uint32), ("grid", C.c_uint32),
-                ("items", C.c_uint32), ("segments", C.c_uint32), ("smem_bytes", C.c_uint32)]
+                ("items", C.c_uint32), ("segments", C.c_uint32), ("smem_bytes", C.c_uint32),
+                ("kernel", C.c_uint32), ("frontier_nodes", C.c_uint32), ("kernels", C.c_uint32)]
+
+
+KERNEL_AUTO, KERNEL_CTA, KERNEL_WARP = 0, 1, 2
 
 
 _lib = None
@@ -111,6 +116,8 @@ def lib():
             "mg_batch_destroy": ([vp], C.c_int),
             "mg_batch_set_keys": ([vp, C.POINTER(vp), C.POINTER(u8p), C.POINTER(sz), C.c_uint32], C.c_int),
             "mg_batch_set_shape": ([vp, C.c_uint32, C.c_uint32], C.c_int),
+            "mg_batch_set_kernel": ([vp, C.c_int], C.c_int),
+            "mg_batch_autotune": ([vp, C.c_uint32, C.POINTER(PlanInfo), C.POINTER(C.c_double)], C.c_int),
             "mg_batch_launch": ([vp, vp], C.c_int),
             "mg_batch_launch_graph": ([vp, vp], C.c_int),
             "mg_batch_read": ([vp, u8p, vp], C.c_int),

@@ -6,6 +6,8 @@
 // (table, domain), key groups, tile depth), persistent device workspaces,
 // CUDA-graph replay, and host deadlines instead of unbounded waits.
 #include <algorithm>
+#include <array>
+#include <map>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -137,7 +139,10 @@ struct mg_context {
   std::mutex mu;              // serialises the one-call path (mg_scan)
   std::mutex attr_mu;         // kernel attribute setup
   size_t prepared_smem[9] = {0};
+  size_t prepared_warp[5][6] = {};
   mg_batch* internal = nullptr;
+  std::mutex tune_mu;  // tuned launch shapes per workload signature
+  std::map<std::string, std::array<uint32_t, 3>> tuned;  // {kind, subtree_bits, keys_per_item}
 };
 
 struct mg_table {
@@ -151,11 +156,18 @@ struct mg_table {
 
 struct mg_batch {
   struct Launch {
-    mg::ScanParams p;
-    uint32_t grid = 0;
+    int kind = MG_KERNEL_CTA;
+    mg::ScanParams p;      // CTA kernel parameters
+    mg::WarpScanParams w;  // warp kernel parameters
+    std::vector<mg::FrontierStep> steps;  // warp kernel: frontier chain, in order
+    std::vector<uint32_t> step_keys;      // keys (grid.y) of each chain step
+    uint32_t grid = 0;     // CTAs
+    uint32_t nparts = 0;   // partial rows (CTAs or warps)
+    uint32_t cols = 0;
     size_t smem = 0;
     int G = 1;
-    uint32_t col0 = 0;  // first share column of this launch
+    uint32_t VT = 0;
+    uint32_t col0 = 0;     // first share column of this launch
   };
   mg_context* ctx = nullptr;
   int device = 0;
@@ -169,12 +181,24 @@ struct mg_batch {
   uint4* d_out = nullptr;
   uint8_t* h_out = nullptr;
   size_t cap_out = 0;
+  uint4* d_fr_seed = nullptr;  // frontier nodes of every warp-kernel key
+  uint8_t* d_fr_t = nullptr;
+  size_t cap_fr = 0;
+  uint4* d_tmp_seed[2] = {nullptr, nullptr};  // frontier chain intermediates
+  uint8_t* d_tmp_t[2] = {nullptr, nullptr};
+  size_t cap_tmp = 0;
   std::vector<Launch> launches;
   uint32_t total_cols = 0;
   std::vector<uint32_t> key_col;    // first share column of input key i
   std::vector<uint32_t> key_bytes;  // share bytes of input key i
   size_t total_share_bytes = 0;
-  uint32_t shape_S = 0, shape_G = 0;
+  uint32_t shape_S = 0, shape_G = 0;  // pinned by mg_batch_set_shape (0 = planner)
+  int kind_pref = MG_KERNEL_AUTO;     // pinned by mg_batch_set_kernel
+  uint32_t eff_S = 0, eff_G = 0;      // shape used by the current plan
+  int eff_kind = MG_KERNEL_AUTO;
+  std::vector<KeyDev> in_keys;        // parsed keys of the current pass, input order
+  std::vector<const mg_table*> in_tables;
+  std::string signature;              // workload signature for the tuned-shape cache
   mg_plan_info info{};
   bool planned = false;
   bool launched = false;
@@ -198,7 +222,36 @@ int prepare_g(mg_context* ctx, int G, size_t smem) {
   return MG_OK;
 }
 
-int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4) {
+int vt_index(uint32_t VT) {
+  int i = 0;
+  while ((1u << i) < VT) ++i;
+  return i;  // 1,2,4,...,32 -> 0..5
+}
+
+int prepare_warp(mg_context* ctx, int G, uint32_t VT, size_t smem) {
+  std::lock_guard<std::mutex> lk(ctx->attr_mu);
+  size_t& have = ctx->prepared_warp[G][vt_index(VT)];
+  if (have >= smem) return MG_OK;
+  MG_CUDA(mg::warp_prepare(G, VT, smem));
+  have = smem;
+  return MG_OK;
+}
+
+template <class T>
+int grow_dev(T*& p, size_t& cap, size_t need, const char* what) {
+  if (need <= cap) return MG_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  if (cudaMalloc(&p, need * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MG_ENOMEM, "cannot allocate %zu bytes of %s", need * sizeof(T), what);
+  }
+  cap = need;
+  return MG_OK;
+}
+
+int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4, size_t fr_nodes, size_t tmp_nodes) {
   if (nkeys > b->cap_keys) {
     if (b->d_keys) cudaFree(b->d_keys);
     if (b->h_keys) cudaFreeHost(b->h_keys);
@@ -212,16 +265,7 @@ int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4) {
     }
     b->cap_keys = nkeys;
   }
-  if (partial_u4 > b->cap_partial) {
-    if (b->d_partial) cudaFree(b->d_partial);
-    b->d_partial = nullptr;
-    b->cap_partial = 0;
-    if (cudaMalloc(&b->d_partial, partial_u4 * 16) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(MG_ENOMEM, "cannot allocate %zu-byte partial buffer", partial_u4 * 16);
-    }
-    b->cap_partial = partial_u4;
-  }
+  if (int rc = grow_dev(b->d_partial, b->cap_partial, partial_u4, "partial rows")) return rc;
   if (out_u4 > b->cap_out) {
     if (b->d_out) cudaFree(b->d_out);
     if (b->h_out) cudaFreeHost(b->h_out);
@@ -235,6 +279,20 @@ int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4) {
     }
     b->cap_out = out_u4;
   }
+  if (fr_nodes > b->cap_fr) {
+    size_t c1 = b->cap_fr, c2 = b->cap_fr;
+    if (int rc = grow_dev(b->d_fr_seed, c1, fr_nodes, "frontier seeds")) return rc;
+    if (int rc = grow_dev(b->d_fr_t, c2, fr_nodes, "frontier control bits")) return rc;
+    b->cap_fr = fr_nodes;
+  }
+  if (tmp_nodes > b->cap_tmp) {
+    for (int i = 0; i < 2; ++i) {
+      size_t c1 = b->cap_tmp, c2 = b->cap_tmp;
+      if (int rc = grow_dev(b->d_tmp_seed[i], c1, tmp_nodes, "frontier chain")) return rc;
+      if (int rc = grow_dev(b->d_tmp_t[i], c2, tmp_nodes, "frontier chain")) return rc;
+    }
+    b->cap_tmp = tmp_nodes;
+  }
   return MG_OK;
 }
 
@@ -243,18 +301,23 @@ struct SegPlan {
   uint32_t d;
   std::vector<uint32_t> keys;  // input key indices, group-major
   uint32_t g;
+  bool warp;
 };
 
-// Heuristic launch shape.  Keys per CTA: rows of up to 128 B leave the pass
-// bound by ChaCha8 issue slots, so one key per CTA maximises occupancy (row
-// re-reads of sibling CTAs hit L2); wider rows share each row load across up
-// to 4 keys.  Tile depth: the deepest in [8, 14] that still gives at least
-// four waves of work items.
-int choose_g(uint32_t V, size_t nkeys, uint32_t pinned) {
+// Keys evaluated together on one work item.  Rows of up to 128 B leave the
+// pass bound by ChaCha8 issue slots, so one key per item maximises the
+// number of independent items (re-reads of a row by sibling items hit L2);
+// wider rows share each row load across up to 4 keys.
+int choose_g(uint32_t V, size_t nkeys, uint32_t pinned, bool warp) {
   int g = pinned ? (int)pinned : (V <= 8 ? 1 : 4);
+  if (warp && g > 4) g = 4;
   if ((size_t)g > nkeys) g = (int)nkeys;
   if (g < 1) g = 1;
-  while (!mg::scan_g_supported(g)) --g;
+  if (warp) {
+    while (!mg::warp_g_supported(g)) --g;
+  } else {
+    while (!mg::scan_g_supported(g)) --g;
+  }
   return g;
 }
 
@@ -263,6 +326,8 @@ void shape_for(uint32_t d, uint32_t S_target, uint32_t& S, uint32_t& U, uint32_t
   U = S >= 1 ? std::min<uint32_t>(8u, S - 1) : 0u;
   M = S - U;
 }
+
+uint64_t ceil_shift(uint64_t x, uint32_t s) { return s >= 64 ? (x ? 1 : 0) : (x + (1ull << s) - 1) >> s; }
 
 }  // namespace
 
@@ -514,6 +579,12 @@ int mg_batch_destroy(mg_batch* b) {
   if (b->d_partial) cudaFree(b->d_partial);
   if (b->d_out) cudaFree(b->d_out);
   if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->d_fr_seed) cudaFree(b->d_fr_seed);
+  if (b->d_fr_t) cudaFree(b->d_fr_t);
+  for (int i = 0; i < 2; ++i) {
+    if (b->d_tmp_seed[i]) cudaFree(b->d_tmp_seed[i]);
+    if (b->d_tmp_t[i]) cudaFree(b->d_tmp_t[i]);
+  }
   for (cudaEvent_t e : {b->ev_k0, b->ev_km, b->ev_k1, b->ev_done, b->ev_h0, b->ev_h1})
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -531,6 +602,387 @@ int mg_batch_set_shape(mg_batch* b, uint32_t subtree_bits, uint32_t keys_per_cta
   return MG_OK;
 }
 
+int mg_batch_set_kernel(mg_batch* b, int kind) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (kind != MG_KERNEL_AUTO && kind != MG_KERNEL_CTA && kind != MG_KERNEL_WARP)
+    return fail(MG_EINVAL, "unknown kernel kind %d", kind);
+  b->kind_pref = kind;
+  return MG_OK;
+}
+
+namespace {
+
+// Plan one CTA-kernel launch over segs (at most kMaxSegs): tile depth S, the
+// deepest in [8, 14] that still gives >= 4 waves of items (or the pinned one).
+int plan_cta(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t col0, size_t& key_cursor,
+             std::vector<uint32_t>& key_col, std::vector<uint32_t>& key_bytes, std::vector<uint32_t>& key_slot,
+             mg_batch::Launch& out) {
+  mg_context* ctx = b->ctx;
+  for (uint32_t S_target = b->eff_S ? b->eff_S : 14;; --S_target) {
+    mg_batch::Launch L;
+    std::memset(&L.p, 0, sizeof L.p);
+    L.kind = MG_KERNEL_CTA;
+    L.G = G;
+    L.col0 = col0;
+    uint32_t slots = 2, cols = 0;
+    uint64_t items = 0;
+    size_t cursor = key_cursor;
+    std::vector<std::pair<uint32_t, uint32_t>> assign;  // (key, column)
+    for (size_t si = 0; si < segs.size(); ++si) {
+      const SegPlan& sp = segs[si];
+      mg::Segment& sg = L.p.seg[si];
+      uint32_t S, U, M;
+      shape_for(sp.d, S_target, S, U, M);
+      sg.table = reinterpret_cast<const uint4*>(sp.table->d);
+      sg.rows = sp.table->rows;
+      sg.V = sp.table->row_bytes / 16;
+      sg.d = sp.d;
+      sg.S = S;
+      sg.U = U;
+      sg.M = M;
+      sg.g = sp.g;
+      sg.groups = (uint32_t)(sp.keys.size() / sp.g);
+      sg.tiles = (uint32_t)ceil_shift(sp.table->rows, S);
+      sg.item_begin = items;
+      sg.key_base = (uint32_t)cursor;
+      sg.col_base = cols;
+      for (size_t j = 0; j < sp.keys.size(); ++j) {
+        key_col[sp.keys[j]] = col0 + cols + (uint32_t)j * sg.V;
+        key_bytes[sp.keys[j]] = sp.table->row_bytes;
+        key_slot[sp.keys[j]] = (uint32_t)(cursor + j);
+      }
+      cursor += sp.keys.size();
+      items += (uint64_t)sg.tiles * sg.groups;
+      cols += (uint32_t)sp.keys.size() * sg.V;
+      slots = std::max(slots, M);
+    }
+    L.p.nsegs = (uint32_t)segs.size();
+    L.p.items = items;
+    L.p.cols = cols;
+    L.p.slots = slots;
+    L.cols = cols;
+    L.smem = mg::scan_smem_bytes(G, slots);
+    int occ = 0;
+    if (L.smem <= ctx->smem_optin) {
+      if (int rc = prepare_g(ctx, G, L.smem)) return rc;
+      occ = mg::scan_occupancy(G, L.smem);
+    }
+    const uint64_t slots_total = (uint64_t)std::max(occ, 1) * ctx->sms;
+    const bool enough = occ > 0 && items >= 4 * slots_total;
+    if (b->eff_S || enough || S_target <= 8) {
+      if (occ <= 0) return fail(MG_EINVAL, "launch shape S=%u G=%d does not fit the device", S_target, G);
+      L.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(items, slots_total));
+      L.nparts = L.grid;
+      key_cursor = cursor;
+      out = std::move(L);
+      return MG_OK;
+    }
+  }
+}
+
+// Plan one warp-kernel launch over segs (same V, at most kMaxSegs): depth-first
+// levels per lane M, chosen for load balance across the persistent warps (the
+// deepest M whose item count splits within 3% of even), or pinned as
+// subtree_bits = M + 5.
+int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT, uint32_t col0,
+              size_t& key_cursor, std::vector<uint32_t>& key_col, std::vector<uint32_t>& key_bytes,
+              std::vector<uint32_t>& key_slot, uint64_t& fr_cursor, size_t& tmp_need, mg_batch::Launch& out) {
+  mg_context* ctx = b->ctx;
+  struct Cand { uint32_t M; double bal; uint64_t items; int occ; size_t smem; };
+  std::vector<Cand> cands;
+  const uint32_t pinned = b->eff_S;
+  for (uint32_t Mt = 10; Mt >= 1; --Mt) {
+    if (pinned && !(pinned >= 6 ? Mt == pinned - 5 : Mt == 1)) continue;
+    uint64_t items = 0;
+    uint32_t slots = 1;
+    for (const SegPlan& sp : segs) {
+      const uint32_t M = std::min(Mt, sp.d);
+      const uint64_t nF = ceil_shift(sp.table->rows, M);
+      items += (sp.keys.size() / sp.g) * ((nF + 31) / 32);
+      slots = std::max(slots, M);
+    }
+    const size_t smem = mg::warp_smem_bytes(G, slots);
+    if (smem > ctx->smem_optin) continue;
+    if (int rc = prepare_warp(ctx, G, VT, smem)) return rc;
+    const int occ = mg::warp_occupancy(G, VT, smem);
+    if (occ <= 0) continue;
+    const uint64_t nw = (uint64_t)occ * ctx->sms * mg::kWarps;
+    const uint64_t per = (items + nw - 1) / nw;
+    const double bal = per ? (double)items / ((double)per * (double)nw) : 1.0;
+    cands.push_back({Mt, bal, items, occ, smem});
+  }
+  if (cands.empty()) return fail(MG_EINVAL, "no warp-kernel shape fits the device (G=%d)", G);
+  const Cand* best = nullptr;
+  for (const Cand& c : cands)
+    if (c.bal >= 0.97) { best = &c; break; }  // deepest balanced
+  if (!best) {
+    best = &cands[0];
+    for (const Cand& c : cands)
+      if (c.bal > best->bal + 0.01) best = &c;
+  }
+
+  mg_batch::Launch L;
+  std::memset(&L.w, 0, sizeof L.w);
+  L.kind = MG_KERNEL_WARP;
+  L.G = G;
+  L.VT = VT;
+  L.col0 = col0;
+  uint64_t items = 0;
+  uint32_t cols = 0, slots = 1;
+  size_t cursor = key_cursor;
+  for (size_t si = 0; si < segs.size(); ++si) {
+    const SegPlan& sp = segs[si];
+    mg::WarpSeg& sg = L.w.seg[si];
+    const uint32_t M = std::min(best->M, sp.d);
+    const uint64_t nF = ceil_shift(sp.table->rows, M);
+    const uint32_t nk = (uint32_t)sp.keys.size();
+    sg.table = reinterpret_cast<const uint4*>(sp.table->d);
+    sg.rows = sp.table->rows;
+    sg.item_begin = items;
+    sg.fr_base = fr_cursor;
+    sg.nF = nF;
+    sg.tiles = (uint32_t)((nF + 31) / 32);
+    sg.groups = nk / sp.g;
+    sg.d = sp.d;
+    sg.M = M;
+    sg.g = sp.g;
+    sg.key_base = (uint32_t)cursor;
+    sg.col_base = cols;
+    for (uint32_t j = 0; j < nk; ++j) {
+      key_col[sp.keys[j]] = col0 + cols + j * VT;
+      key_bytes[sp.keys[j]] = sp.table->row_bytes;
+      key_slot[sp.keys[j]] = (uint32_t)(cursor + j);
+    }
+    // Frontier chain: levels 0 -> F = d - M in steps of at most 8 levels.
+    const uint32_t F = sp.d - M;
+    const uint32_t nsteps = F ? (F + 7) / 8 : 1;
+    uint32_t Lv = 0;
+    for (uint32_t st = 0; st < nsteps; ++st) {
+      mg::FrontierStep f;
+      std::memset(&f, 0, sizeof f);
+      const uint32_t c = F ? (st == 0 ? F - 8 * (nsteps - 1) : 8u) : 0u;
+      f.L_in = Lv;
+      f.c = c;
+      f.n_in = Lv ? ceil_shift(sp.table->rows, sp.d - Lv) : 1;
+      f.n_out = ceil_shift(sp.table->rows, sp.d - (Lv + c));
+      const bool last = st + 1 == nsteps;
+      f.out_base = last ? fr_cursor : 0;
+      f.out_stride = last ? nF : f.n_out;
+      if (!last) tmp_need = std::max<size_t>(tmp_need, (size_t)nk * f.n_out);
+      f.keys = nullptr;  // set after allocation (key_base offset kept in in_t slot below)
+      L.steps.push_back(f);
+      L.step_keys.push_back(nk);
+      Lv += c;
+    }
+    fr_cursor += (uint64_t)nk * nF;
+    cursor += nk;
+    items += (uint64_t)sg.groups * sg.tiles;
+    cols += nk * VT;
+    slots = std::max(slots, M);
+  }
+  L.w.nsegs = (uint32_t)segs.size();
+  L.w.items = items;
+  L.w.cols = cols;
+  L.w.slots = slots;
+  L.cols = cols;
+  L.smem = mg::warp_smem_bytes(G, slots);
+  if (int rc = prepare_warp(ctx, G, VT, L.smem)) return rc;
+  const int occ = mg::warp_occupancy(G, VT, L.smem);
+  if (occ <= 0) return fail(MG_EINVAL, "warp kernel does not fit the device");
+  const uint64_t nctas = (uint64_t)occ * ctx->sms;
+  const uint64_t need_ctas = (items + mg::kWarps - 1) / mg::kWarps;
+  L.grid = (uint32_t)std::max<uint64_t>(1, std::min(nctas, need_ctas));
+  L.nparts = L.grid * mg::kWarps;
+  key_cursor = cursor;
+  out = std::move(L);
+  return MG_OK;
+}
+
+}  // namespace
+
+// mark: event recorded after the last scan launch (before its reduction),
+// so that the scan kernels can be timed apart from the reductions.
+static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
+  for (size_t i = 0; i < b->launches.size(); ++i) {
+    const mg_batch::Launch& L = b->launches[i];
+    if (L.kind == MG_KERNEL_CTA) {
+      MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
+    } else {
+      for (size_t k = 0; k < L.steps.size(); ++k) MG_CUDA(mg::launch_frontier(L.steps[k], L.step_keys[k], st));
+      MG_CUDA(mg::launch_scan_warp(L.G, L.VT, L.w, L.grid, L.smem, st));
+    }
+    if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
+    MG_CUDA(mg::launch_reduce(b->d_partial, L.nparts, L.cols, b->d_out + L.col0, st));
+  }
+  return MG_OK;
+}
+
+namespace {
+
+// Plan the pass for b->in_keys / b->in_tables with the effective shape
+// (b->eff_kind, b->eff_S, b->eff_G), allocate, stage the keys and copy them
+// to the device on the workspace stream.
+int plan_pass(mg_batch* b) {
+  mg_context* ctx = b->ctx;
+  const uint32_t nkeys = (uint32_t)b->in_keys.size();
+  std::vector<KeyDev>& parsed = b->in_keys;
+  std::vector<SegPlan> segs;
+  for (uint32_t i = 0; i < nkeys; ++i) {
+    const mg_table* t = b->in_tables[i];
+    const uint32_t d = parsed[i].domain_bits;
+    auto it = std::find_if(segs.begin(), segs.end(),
+                           [&](const SegPlan& s) { return s.table == t && s.d == d; });
+    if (it == segs.end()) {
+      segs.push_back(SegPlan{t, d, {}, 1, false});
+      it = segs.end() - 1;
+    }
+    it->keys.push_back(i);
+  }
+
+  // Kernel per segment: the warp kernel for rows of 16..512 B (V dividing
+  // 32) and d >= 1, the CTA kernel otherwise.
+  for (SegPlan& sp : segs) {
+    const uint32_t V = sp.table->row_bytes / 16;
+    const bool ok = mg::warp_vt_supported(V) && sp.d >= 1;
+    if (b->eff_kind == MG_KERNEL_WARP && !ok)
+      return fail(MG_EINVAL, "the warp kernel needs row_bytes in {16..512, powers of two} and d >= 1");
+    sp.warp = ok && b->eff_kind != MG_KERNEL_CTA;
+  }
+  uint32_t Vc = 1, Vw = 1;
+  size_t nc = 1, nwk = 1;
+  for (const SegPlan& sp : segs) {
+    const uint32_t V = sp.table->row_bytes / 16;
+    if (sp.warp) { Vw = std::max(Vw, V); nwk = std::max(nwk, sp.keys.size()); }
+    else { Vc = std::max(Vc, V); nc = std::max(nc, sp.keys.size()); }
+  }
+  const int Gc = choose_g(Vc, nc, b->eff_G, false);
+  const int Gw = choose_g(Vw, nwk, b->eff_G, true);
+  std::vector<SegPlan> split;
+  for (SegPlan& sp : segs) {
+    const int G = sp.warp ? Gw : Gc;
+    const uint32_t g = (uint32_t)std::min<size_t>((size_t)G, sp.keys.size());
+    const size_t full = sp.keys.size() / g * g;
+    split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin(), sp.keys.begin() + full), g, sp.warp});
+    if (full < sp.keys.size())
+      split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin() + full, sp.keys.end()),
+                              (uint32_t)(sp.keys.size() - full), sp.warp});
+  }
+
+  // Launches: CTA-kernel segments in chunks of kMaxSegs; warp-kernel segments
+  // grouped by V, then chunks of kMaxSegs.
+  std::vector<mg_batch::Launch> launches;
+  std::vector<uint32_t> key_col(nkeys), key_bytes(nkeys), key_slot(nkeys);
+  size_t key_cursor = 0, tmp_need = 0;
+  uint64_t fr_cursor = 0;
+  uint32_t total_cols = 0;
+  std::vector<SegPlan> cta_segs;
+  for (const SegPlan& sp : split)
+    if (!sp.warp) cta_segs.push_back(sp);
+  for (size_t s0 = 0; s0 < cta_segs.size(); s0 += mg::kMaxSegs) {
+    std::vector<SegPlan> chunk(cta_segs.begin() + s0,
+                               cta_segs.begin() + std::min(cta_segs.size(), s0 + mg::kMaxSegs));
+    mg_batch::Launch L;
+    if (int rc = plan_cta(b, chunk, Gc, total_cols, key_cursor, key_col, key_bytes, key_slot, L)) return rc;
+    total_cols += L.cols;
+    launches.push_back(std::move(L));
+  }
+  for (uint32_t VT = 1; VT <= 32; VT *= 2) {
+    std::vector<SegPlan> ws;
+    for (const SegPlan& sp : split)
+      if (sp.warp && sp.table->row_bytes / 16 == VT) ws.push_back(sp);
+    for (size_t s0 = 0; s0 < ws.size(); s0 += mg::kMaxSegs) {
+      std::vector<SegPlan> chunk(ws.begin() + s0, ws.begin() + std::min(ws.size(), s0 + mg::kMaxSegs));
+      mg_batch::Launch L;
+      if (int rc = plan_warp(b, chunk, Gw, VT, total_cols, key_cursor, key_col, key_bytes, key_slot, fr_cursor,
+                             tmp_need, L))
+        return rc;
+      total_cols += L.cols;
+      launches.push_back(std::move(L));
+    }
+  }
+
+  size_t max_partial = 0;
+  for (const mg_batch::Launch& L : launches) max_partial = std::max(max_partial, (size_t)L.nparts * L.cols);
+  if (int rc = grow(b, nkeys, max_partial, total_cols, (size_t)fr_cursor, tmp_need)) return rc;
+  for (uint32_t i = 0; i < nkeys; ++i) b->h_keys[key_slot[i]] = parsed[i];
+  for (mg_batch::Launch& L : launches) {
+    if (L.kind == MG_KERNEL_CTA) {
+      L.p.keys = b->d_keys;
+      L.p.partial = b->d_partial;
+      continue;
+    }
+    L.w.keys = b->d_keys;
+    L.w.fr_seed = b->d_fr_seed;
+    L.w.fr_t = b->d_fr_t;
+    L.w.partial = b->d_partial;
+    // Wire the frontier chains: each segment's steps are consecutive.
+    size_t st = 0;
+    for (uint32_t si = 0; si < L.w.nsegs; ++si) {
+      const mg::WarpSeg& sg = L.w.seg[si];
+      const uint32_t F = sg.d - sg.M;
+      const uint32_t nsteps = F ? (F + 7) / 8 : 1;
+      for (uint32_t k = 0; k < nsteps; ++k, ++st) {
+        mg::FrontierStep& f = L.steps[st];
+        f.keys = b->d_keys + sg.key_base;
+        f.in_seed = k ? b->d_tmp_seed[(k - 1) & 1] : nullptr;
+        f.in_t = k ? b->d_tmp_t[(k - 1) & 1] : nullptr;
+        const bool last = k + 1 == nsteps;
+        f.out_seed = last ? b->d_fr_seed : b->d_tmp_seed[k & 1];
+        f.out_t = last ? b->d_fr_t : b->d_tmp_t[k & 1];
+      }
+    }
+  }
+  MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * sizeof(KeyDev), cudaMemcpyHostToDevice,
+                          b->stream));
+  b->launches = std::move(launches);
+  b->total_cols = total_cols;
+  b->key_col = std::move(key_col);
+  b->key_bytes = std::move(key_bytes);
+  b->total_share_bytes = 0;
+  for (uint32_t i = 0; i < nkeys; ++i) b->total_share_bytes += b->key_bytes[i];
+  const mg_batch::Launch& L0 = b->launches[0];
+  b->info.kernel = (uint32_t)L0.kind;
+  b->info.keys_per_cta = (uint32_t)L0.G;
+  b->info.grid = L0.grid;
+  b->info.items = (uint32_t)(L0.kind == MG_KERNEL_CTA ? L0.p.items : L0.w.items);
+  b->info.segments = (uint32_t)split.size();
+  b->info.smem_bytes = (uint32_t)L0.smem;
+  b->info.subtree_bits = 0;
+  for (const mg_batch::Launch& L : b->launches) {
+    if (L.kind == MG_KERNEL_CTA)
+      for (uint32_t s = 0; s < L.p.nsegs; ++s) b->info.subtree_bits = std::max(b->info.subtree_bits, L.p.seg[s].S);
+    else
+      for (uint32_t s = 0; s < L.w.nsegs; ++s) b->info.subtree_bits = std::max(b->info.subtree_bits, L.w.seg[s].M + 5);
+  }
+  b->info.frontier_nodes = (uint32_t)std::min<uint64_t>(fr_cursor, 0xFFFFFFFFu);
+  b->info.kernels = 0;
+  for (const mg_batch::Launch& L : b->launches) b->info.kernels += 2 + (uint32_t)L.steps.size();
+  b->planned = true;
+  return MG_OK;
+}
+
+// Workload signature: the (rows, row bytes, depth, keys) of every segment.
+std::string signature_of(const mg_batch* b) {
+  std::vector<std::array<uint64_t, 4>> segs;
+  for (size_t i = 0; i < b->in_keys.size(); ++i) {
+    const mg_table* t = b->in_tables[i];
+    const uint64_t d = b->in_keys[i].domain_bits;
+    bool found = false;
+    for (auto& s : segs)
+      if (s[0] == (uint64_t)t->rows && s[1] == t->row_bytes && s[2] == d && !found) {
+        ++s[3];
+        found = true;
+      }
+    if (!found) segs.push_back({(uint64_t)t->rows, t->row_bytes, d, 1});
+  }
+  std::string sig = std::to_string(b->ctx->sms);
+  for (auto& s : segs)
+    for (uint64_t v : s) sig += ":" + std::to_string(v);
+  return sig;
+}
+
+}  // namespace
+
 int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t* const* keys,
                       const size_t* key_lens, uint32_t nkeys) {
   if (!b || !tables || !keys || !key_lens) return fail(MG_EINVAL, "null argument");
@@ -540,10 +992,8 @@ int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t*
     return fail(MG_EBUSY, "workspace still owns a pass in flight");
   cudaGetLastError();
   mg_context* ctx = b->ctx;
-
-  // Parse keys and group them into (table, domain) segments.
   std::vector<KeyDev> parsed(nkeys);
-  std::vector<SegPlan> segs;
+  std::vector<const mg_table*> tabs(nkeys);
   for (uint32_t i = 0; i < nkeys; ++i) {
     const mg_table* t = tables[i];
     if (!t) return fail(MG_EINVAL, "null table for key %u", i);
@@ -553,152 +1003,113 @@ int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t*
     if (t->rows > domain_size(d))
       return fail(MG_ERANGE, "more rows than domain size: %llu rows, key %u has %u domain bits",
                   (unsigned long long)t->rows, i, d);
-    auto it = std::find_if(segs.begin(), segs.end(),
-                           [&](const SegPlan& s) { return s.table == t && s.d == d; });
-    if (it == segs.end()) {
-      segs.push_back(SegPlan{t, d, {}, 1});
-      it = segs.end() - 1;
-    }
-    it->keys.push_back(i);
+    tabs[i] = t;
   }
-
-  // Keys per CTA from the widest-row segment with the most keys; split
-  // segments whose key count is not a multiple of it.
-  uint32_t Vmax = 1;
-  size_t nmax = 1;
-  for (const SegPlan& s : segs) {
-    Vmax = std::max(Vmax, s.table->row_bytes / 16);
-    nmax = std::max(nmax, s.keys.size());
-  }
-  const int G = choose_g(Vmax, nmax, b->shape_G);
-  std::vector<SegPlan> split;
-  for (SegPlan& s : segs) {
-    const uint32_t g = (uint32_t)std::min<size_t>((size_t)G, s.keys.size());
-    const size_t full = s.keys.size() / g * g;
-    SegPlan a{s.table, s.d, std::vector<uint32_t>(s.keys.begin(), s.keys.begin() + full), g};
-    split.push_back(a);
-    if (full < s.keys.size()) {
-      SegPlan r{s.table, s.d, std::vector<uint32_t>(s.keys.begin() + full, s.keys.end()),
-                (uint32_t)(s.keys.size() - full)};
-      split.push_back(r);
+  b->in_keys = std::move(parsed);
+  b->in_tables = std::move(tabs);
+  b->signature = signature_of(b);
+  // Effective shape: what the caller pinned, else a tuned shape for this
+  // workload, else the planner's heuristics.
+  b->eff_kind = b->kind_pref;
+  b->eff_S = b->shape_S;
+  b->eff_G = b->shape_G;
+  if (b->kind_pref == MG_KERNEL_AUTO && b->shape_S == 0 && b->shape_G == 0) {
+    std::lock_guard<std::mutex> lk(ctx->tune_mu);
+    auto it = ctx->tuned.find(b->signature);
+    if (it != ctx->tuned.end()) {
+      b->eff_kind = (int)it->second[0];
+      b->eff_S = it->second[1];
+      b->eff_G = it->second[2];
     }
   }
-
-  // Choose the tile depth: the deepest that still yields >= 4 waves.
-  const uint32_t S_candidates_hi = 14, S_candidates_lo = 8;
-  uint32_t S_target = b->shape_S ? b->shape_S : S_candidates_hi;
-  std::vector<mg_batch::Launch> launches;
-  uint32_t total_cols = 0;
-  std::vector<uint32_t> key_col(nkeys), key_bytes(nkeys), key_slot(nkeys);
-  size_t max_partial = 0;
-  for (;;) {
-    launches.clear();
-    total_cols = 0;
-    max_partial = 0;
-    uint64_t total_items = 0;
-    size_t key_cursor = 0;
-    for (size_t s0 = 0; s0 < split.size(); s0 += mg::kMaxSegs) {
-      mg_batch::Launch L;
-      std::memset(&L.p, 0, sizeof L.p);
-      L.G = G;
-      L.col0 = total_cols;
-      uint32_t slots = 2, cols = 0;
-      uint64_t items = 0;
-      const size_t s1 = std::min(split.size(), s0 + mg::kMaxSegs);
-      for (size_t si = s0; si < s1; ++si) {
-        const SegPlan& sp = split[si];
-        mg::Segment& sg = L.p.seg[si - s0];
-        uint32_t S, U, M;
-        shape_for(sp.d, S_target, S, U, M);
-        sg.table = reinterpret_cast<const uint4*>(sp.table->d);
-        sg.rows = sp.table->rows;
-        sg.V = sp.table->row_bytes / 16;
-        sg.d = sp.d;
-        sg.S = S;
-        sg.U = U;
-        sg.M = M;
-        sg.g = sp.g;
-        sg.groups = (uint32_t)(sp.keys.size() / sp.g);
-        sg.tiles = (uint32_t)((sp.table->rows + (1ull << S) - 1) >> S);
-        sg.item_begin = items;
-        sg.key_base = (uint32_t)key_cursor;
-        sg.col_base = cols;
-        for (size_t j = 0; j < sp.keys.size(); ++j) {
-          const uint32_t ki = sp.keys[j];
-          key_col[ki] = L.col0 + cols + (uint32_t)j * sg.V;
-          key_bytes[ki] = sp.table->row_bytes;
-          key_slot[ki] = (uint32_t)(key_cursor + j);
-        }
-        key_cursor += sp.keys.size();
-        items += (uint64_t)sg.tiles * sg.groups;
-        cols += (uint32_t)sp.keys.size() * sg.V;
-        slots = std::max(slots, M);
-      }
-      L.p.nsegs = (uint32_t)(s1 - s0);
-      L.p.items = items;
-      L.p.cols = cols;
-      L.p.slots = slots;
-      L.smem = mg::scan_smem_bytes(G, slots);
-      launches.push_back(L);
-      total_cols += cols;
-      total_items += items;
-    }
-    // Occupancy of the chosen shape.
-    bool ok = true;
-    uint64_t min_slots = UINT64_MAX;
-    for (mg_batch::Launch& L : launches) {
-      if (L.smem > ctx->smem_optin) { ok = false; break; }
-      if (int rc = prepare_g(ctx, G, L.smem)) return rc;
-      const int occ = mg::scan_occupancy(G, L.smem);
-      if (occ <= 0) { ok = false; break; }
-      const uint64_t slots_total = (uint64_t)occ * ctx->sms;
-      L.grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(L.p.items, slots_total));
-      min_slots = std::min(min_slots, slots_total);
-      max_partial = std::max(max_partial, (size_t)L.grid * L.p.cols);
-    }
-    const bool enough = ok && total_items >= 4 * min_slots;
-    if (b->shape_S || enough || S_target <= S_candidates_lo) {
-      if (!ok) return fail(MG_EINVAL, "launch shape S=%u G=%d does not fit the device", S_target, G);
-      break;
-    }
-    --S_target;
-  }
-
-  if (int rc = grow(b, nkeys, max_partial, total_cols)) return rc;
-  for (uint32_t i = 0; i < nkeys; ++i) b->h_keys[key_slot[i]] = parsed[i];
-  for (mg_batch::Launch& L : launches) {
-    L.p.keys = b->d_keys;
-    L.p.partial = b->d_partial;
-  }
-  MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * sizeof(KeyDev),
-                          cudaMemcpyHostToDevice, b->stream));
-  b->launches = std::move(launches);
-  b->total_cols = total_cols;
-  b->key_col = std::move(key_col);
-  b->key_bytes = std::move(key_bytes);
-  b->total_share_bytes = 0;
-  for (uint32_t i = 0; i < nkeys; ++i) b->total_share_bytes += b->key_bytes[i];
-  b->info.subtree_bits = 0;
-  for (const mg_batch::Launch& L : b->launches)
-    for (uint32_t s = 0; s < L.p.nsegs; ++s) b->info.subtree_bits = std::max(b->info.subtree_bits, L.p.seg[s].S);
-  b->info.keys_per_cta = (uint32_t)G;
-  b->info.grid = b->launches[0].grid;
-  b->info.items = (uint32_t)b->launches[0].p.items;
-  b->info.segments = (uint32_t)split.size();
-  b->info.smem_bytes = (uint32_t)b->launches[0].smem;
-  b->planned = true;
-  return MG_OK;
+  return plan_pass(b);
 }
 
-// mark: event recorded after the last scan launch (before its reduction),
-// so that the scan kernels can be timed apart from the reductions.
-static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
-  for (size_t i = 0; i < b->launches.size(); ++i) {
-    const mg_batch::Launch& L = b->launches[i];
-    MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
-    if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
-    MG_CUDA(mg::launch_reduce(b->d_partial, L.grid, L.p.cols, b->d_out + L.col0, st));
+int mg_batch_autotune(mg_batch* b, uint32_t budget_ms, mg_plan_info* best_info, double* best_ms) {
+  if (!b) return fail(MG_EINVAL, "null workspace");
+  if (!b->planned) return fail(MG_EINVAL, "mg_batch_set_keys has not been called");
+  if (int rc = set_device(b)) return rc;
+  if (b->launched && cudaEventQuery(b->ev_done) == cudaErrorNotReady)
+    return fail(MG_EBUSY, "workspace still owns a pass in flight");
+  cudaGetLastError();
+  struct Cand { int kind; uint32_t S, G; };
+  std::vector<Cand> cands;
+  cands.push_back({MG_KERNEL_AUTO, 0, 0});
+  size_t nk = b->in_keys.size();
+  bool warp_ok = true;
+  for (size_t i = 0; i < nk; ++i)
+    warp_ok = warp_ok && mg::warp_vt_supported(b->in_tables[i]->row_bytes / 16) && b->in_keys[i].domain_bits >= 1;
+  const uint32_t Gs[4] = {1, 2, 3, 4};
+  for (uint32_t G : Gs) {
+    if (G > nk && G != 1) continue;
+    if (warp_ok)
+      for (uint32_t sb = 15; sb >= 6; --sb) cands.push_back({MG_KERNEL_WARP, sb, G});
+    for (uint32_t S = 14; S >= 8; --S) cands.push_back({MG_KERNEL_CTA, S, G});
   }
+  const int save_kind = b->eff_kind;
+  const uint32_t save_S = b->eff_S, save_G = b->eff_G;
+  std::vector<uint8_t> ref, got;
+  double best = 1e300;
+  Cand best_c = cands[0];
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MG_CUDA(cudaEventCreate(&e0));
+  MG_CUDA(cudaEventCreate(&e1));
+  int rc = MG_OK;
+  for (size_t ci = 0; ci < cands.size(); ++ci) {
+    const Cand& c = cands[ci];
+    if (ci > 0 && budget_ms &&
+        std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(budget_ms))
+      break;
+    b->eff_kind = c.kind;
+    b->eff_S = c.S;
+    b->eff_G = c.G;
+    if (plan_pass(b) != MG_OK) continue;  // shape does not fit: skip
+    // Warm-up launch, then the best of three timed launches.
+    if ((rc = enqueue_pass(b, b->stream, nullptr))) break;
+    float ms_best = 1e30f;
+    for (int r = 0; r < 3 && rc == MG_OK; ++r) {
+      cudaEventRecord(e0, b->stream);
+      rc = enqueue_pass(b, b->stream, nullptr);
+      cudaEventRecord(e1, b->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(MG_ECUDA, "autotune launch failed"); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms_best = std::min(ms_best, ms);
+      if (ci > 0 && ms > 4 * best) break;  // clearly worse: stop timing it
+    }
+    if (rc) break;
+    got.resize((size_t)b->total_cols * 16);
+    if (cudaMemcpy(got.data(), b->d_out, got.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      rc = fail(MG_ECUDA, "autotune read-back failed");
+      break;
+    }
+    // Same shares from every shape, compared in input-key order.
+    std::vector<uint8_t> ordered;
+    for (size_t i = 0; i < b->key_col.size(); ++i)
+      ordered.insert(ordered.end(), got.begin() + (size_t)b->key_col[i] * 16,
+                     got.begin() + (size_t)b->key_col[i] * 16 + b->key_bytes[i]);
+    if (ref.empty()) ref = ordered;
+    else if (ordered != ref) { rc = fail(MG_ECUDA, "autotune: shape %d/%u/%u changed the shares", c.kind, c.S, c.G); break; }
+    if (ms_best < best) { best = ms_best; best_c = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    b->eff_kind = save_kind; b->eff_S = save_S; b->eff_G = save_G;
+    plan_pass(b);
+    return rc;
+  }
+  {
+    std::lock_guard<std::mutex> lk(b->ctx->tune_mu);
+    b->ctx->tuned[b->signature] = {(uint32_t)best_c.kind, best_c.S, best_c.G};
+  }
+  b->eff_kind = best_c.kind;
+  b->eff_S = best_c.S;
+  b->eff_G = best_c.G;
+  if ((rc = plan_pass(b))) return rc;
+  if (best_info) *best_info = b->info;
+  if (best_ms) *best_ms = best;
   return MG_OK;
 }
 
@@ -726,9 +1137,20 @@ int mg_batch_launch_graph(mg_batch* b, void* stream) {
   if (int rc = set_device(b)) return rc;
   // Signature: everything baked into the captured kernel nodes.
   std::vector<uint8_t> sig;
+  auto add = [&](const void* p, size_t n) {
+    const uint8_t* q = static_cast<const uint8_t*>(p);
+    sig.insert(sig.end(), q, q + n);
+  };
   for (const mg_batch::Launch& L : b->launches) {
-    const uint8_t* pp = reinterpret_cast<const uint8_t*>(&L);
-    sig.insert(sig.end(), pp, pp + sizeof L);
+    add(&L.kind, sizeof L.kind);
+    add(&L.grid, sizeof L.grid);
+    add(&L.smem, sizeof L.smem);
+    add(&L.G, sizeof L.G);
+    add(&L.VT, sizeof L.VT);
+    add(&L.col0, sizeof L.col0);
+    if (L.kind == MG_KERNEL_CTA) add(&L.p, sizeof L.p);
+    else add(&L.w, sizeof L.w);
+    for (const mg::FrontierStep& f : L.steps) add(&f, sizeof f);
   }
   const uint8_t* op = reinterpret_cast<const uint8_t*>(&b->d_out);
   sig.insert(sig.end(), op, op + sizeof b->d_out);

@@ -106,6 +106,28 @@ __device__ __forceinline__ uint4 leaf_mask(const uint4 s, const uint32_t t, cons
   return make_uint4(s.x ^ (f.x & m), s.y ^ (f.y & m), s.z ^ (f.z & m), s.w ^ (f.w & m));
 }
 
+// Same as expand_cw with the key read through the read-only data path (the
+// key is uniform across a warp, so every load is a broadcast L1 hit).
+__device__ __forceinline__ void expand_cw_g(const uint4 s, const uint32_t t, const KeyDev* __restrict__ k,
+                                            const uint32_t level, uint4& L, uint32_t& tl, uint4& R,
+                                            uint32_t& tr) {
+  const uint4 cw = __ldg(&k->cw_seed[level]);
+  const uint32_t cwl = __ldg(&k->cw_tl[level]);
+  const uint32_t cwr = __ldg(&k->cw_tr[level]);
+  prg_expand(s, L, R, tl, tr);
+  const uint32_t m = (t == 1u) ? 0xFFFFFFFFu : 0u;
+  L.x ^= cw.x & m; L.y ^= cw.y & m; L.z ^= cw.z & m; L.w ^= cw.w & m;
+  R.x ^= cw.x & m; R.y ^= cw.y & m; R.z ^= cw.z & m; R.w ^= cw.w & m;
+  tl ^= cwl & m;
+  tr ^= cwr & m;
+}
+
+__device__ __forceinline__ uint4 leaf_mask_g(const uint4 s, const uint32_t t, const KeyDev* __restrict__ k) {
+  const uint32_t m = (t == 1u) ? 0xFFFFFFFFu : 0u;
+  const uint4 f = __ldg(&k->final_cw);
+  return make_uint4(s.x ^ (f.x & m), s.y ^ (f.y & m), s.z ^ (f.z & m), s.w ^ (f.w & m));
+}
+
 __device__ __forceinline__ uint4 xor_and(uint4 acc, const uint4 d, const uint4 m) {
   acc.x ^= d.x & m.x; acc.y ^= d.y & m.y; acc.z ^= d.z & m.z; acc.w ^= d.w & m.w;
   return acc;
@@ -142,6 +164,60 @@ struct ScanParams {
   uint32_t nsegs;
   uint32_t cols;        // total share uint4s of the pass
   uint32_t slots;       // stack slots per key per thread allocated in smem
+};
+
+// ---- warp-independent scan ------------------------------------------------
+//
+// A frontier holds, for every key, the tree nodes at level F = d - M whose
+// subtrees intersect the table (nF = ceil(rows / 2^M) of them).  A warp work
+// item is 32 consecutive frontier nodes of one key group ("warp tile", 32 x
+// 2^M rows); each lane walks its node's 2^M leaves depth-first.
+
+constexpr int kWarps = kThreads / 32;
+
+struct WarpSeg {
+  const uint4* table;   // rows * V uint4
+  uint64_t rows;
+  uint64_t item_begin;  // first global item of the segment
+  uint64_t fr_base;     // frontier index of the segment's key 0 (key j at fr_base + j * nF)
+  uint64_t nF;          // frontier nodes per key
+  uint32_t tiles;       // warp tiles per key group = ceil(nF / 32)
+  uint32_t groups;      // key groups (items are group-major)
+  uint32_t d;           // domain bits
+  uint32_t M;           // depth-first levels per lane (>= 1)
+  uint32_t g;           // keys per group
+  uint32_t key_base;    // KeyDev index of the segment's key 0
+  uint32_t col_base;    // first share column of the segment
+  uint32_t pad;
+};
+
+struct WarpScanParams {
+  WarpSeg seg[kMaxSegs];
+  const KeyDev* keys;
+  const uint4* fr_seed;
+  const uint8_t* fr_t;
+  uint4* partial;       // [gridDim.x * kWarps][cols]
+  uint64_t items;
+  uint32_t nsegs;
+  uint32_t cols;
+  uint32_t slots;       // depth-first stack slots per key per lane (>= max M)
+};
+
+// One breadth-first step of the frontier chain: every CTA expands one node of
+// level L_in of key blockIdx.y by c <= 8 levels and stores the first n_out
+// nodes of level L_in + c.
+struct FrontierStep {
+  const KeyDev* keys;     // the segment's keys
+  const uint4* in_seed;   // level L_in (unused when L_in == 0): key j at j * n_in
+  const uint8_t* in_t;
+  uint4* out_seed;        // key j at out_base + j * out_stride
+  uint8_t* out_t;
+  uint64_t n_in;
+  uint64_t n_out;
+  uint64_t out_base;
+  uint64_t out_stride;
+  uint32_t L_in;
+  uint32_t c;
 };
 
 }  // namespace mg

@@ -198,6 +198,215 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
   }
 }
 
+// ---- warp-independent path -------------------------------------------------
+
+// Frontier chain step: CTA (node, key) expands node `blockIdx.x` of level
+// L_in of key `blockIdx.y` by c <= 8 levels breadth-first in shared memory
+// and stores the nodes of level L_in + c that intersect the table.
+__global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constant__ FrontierStep f) {
+  __shared__ uint4 sa[kThreads], sb[kThreads];
+  __shared__ uint8_t ta[kThreads], tb[kThreads];
+  const uint32_t tid = threadIdx.x;
+  const uint64_t node = blockIdx.x, j = blockIdx.y;
+  const uint64_t out0 = node << f.c;
+  if (out0 >= f.n_out) return;  // uniform per CTA
+  const KeyDev* __restrict__ K = f.keys + j;
+  if (tid == 0) {
+    if (f.L_in == 0) {
+      sa[0] = __ldg(&K->root_seed);
+      ta[0] = (uint8_t)__ldg(&K->root_t);
+    } else {
+      sa[0] = f.in_seed[j * f.n_in + node];
+      ta[0] = f.in_t[j * f.n_in + node];
+    }
+  }
+  __syncthreads();
+  uint4* cs = sa; uint8_t* ct = ta;
+  uint4* ns = sb; uint8_t* nt = tb;
+  for (uint32_t lv = 0; lv < f.c; ++lv) {
+    if (tid < (1u << lv)) {
+      uint4 Lc, Rc;
+      uint32_t tl, tr;
+      expand_cw_g(cs[tid], ct[tid], K, f.L_in + lv, Lc, tl, Rc, tr);
+      ns[2 * tid] = Lc;
+      ns[2 * tid + 1] = Rc;
+      nt[2 * tid] = (uint8_t)tl;
+      nt[2 * tid + 1] = (uint8_t)tr;
+    }
+    __syncthreads();
+    uint4* x = cs; cs = ns; ns = x;
+    uint8_t* y = ct; ct = nt; nt = y;
+  }
+  const uint32_t n = 1u << f.c;
+  for (uint32_t i = tid; i < n; i += kThreads) {
+    const uint64_t o = out0 + i;
+    if (o < f.n_out) {
+      f.out_seed[f.out_base + j * f.out_stride + o] = cs[i];
+      f.out_t[f.out_base + j * f.out_stride + o] = ct[i];
+    }
+  }
+}
+
+// Warp-independent fused expansion + scan.  Every warp takes a contiguous
+// range of (group, warp tile) items in group-major order, so consecutive
+// items usually belong to the same keys and the accumulators stay in
+// registers; they are flushed (warp shuffle XOR) into the warp's own
+// partial row when the group changes.  Per item each lane loads its
+// frontier node and walks its 2^M leaves depth-first (stack in the warp's
+// shared-memory slice); a step yields one leaf pair per lane for every key,
+// exchanged through shared memory with __syncwarp only, and the warp scans
+// the step's 64 rows (32 runs of 2) with 128-bit loads issued before the
+// ChaCha work.  V = VT uint4 per row (VT divides 32, so a lane always holds
+// the same 16-byte position of a row).
+#ifndef MG_WARP_MIN_BLOCKS
+#define MG_WARP_MIN_BLOCKS 2
+#endif
+#ifndef MG_WARP_PREFETCH
+#define MG_WARP_PREFETCH 8
+#endif
+
+template <int G, int VT>
+__global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t slots = p.slots;
+  uint4* const base4 = reinterpret_cast<uint4*>(smem_raw);
+  uint4* const w_mask = base4 + (size_t)warp * G * 64;                                  // [G][64]
+  uint4* const w_seed = base4 + (size_t)kWarps * G * 64 + (size_t)warp * G * slots * 32;  // [G][slots][32]
+  uint8_t* const w_t = reinterpret_cast<uint8_t*>(base4 + (size_t)kWarps * G * 64 + (size_t)kWarps * G * slots * 32) +
+                       (size_t)warp * G * slots * 32;
+
+  const uint64_t gw = (uint64_t)blockIdx.x * kWarps + warp;
+  const uint64_t nw = (uint64_t)gridDim.x * kWarps;
+  uint4* const my_partial = p.partial + gw * p.cols;
+  for (uint32_t c = lane; c < p.cols; c += 32) my_partial[c] = make_uint4(0u, 0u, 0u, 0u);
+  __syncwarp();
+
+  constexpr int NL = 2 * VT;            // uint4 loads per lane per step
+  constexpr int PF = NL < MG_WARP_PREFETCH ? NL : MG_WARP_PREFETCH;  // loads issued before the ChaCha work
+  constexpr uint32_t RPL = 32 / VT;     // rows covered by one warp-wide load
+  const uint32_t pos = lane % VT, r0 = lane / VT;
+
+  uint4 acc[G];
+#pragma unroll
+  for (int k = 0; k < G; ++k) acc[k] = make_uint4(0u, 0u, 0u, 0u);
+  int cur_seg = -1;
+  uint32_t cur_group = 0;
+
+  auto flush = [&](const WarpSeg& sg, uint32_t group) {
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+      uint4 v = acc[k];
+#pragma unroll
+      for (uint32_t off = 16; off >= (uint32_t)VT; off >>= 1) {
+        v.x ^= __shfl_xor_sync(0xFFFFFFFFu, v.x, off);
+        v.y ^= __shfl_xor_sync(0xFFFFFFFFu, v.y, off);
+        v.z ^= __shfl_xor_sync(0xFFFFFFFFu, v.z, off);
+        v.w ^= __shfl_xor_sync(0xFFFFFFFFu, v.w, off);
+      }
+      if ((uint32_t)k < sg.g && lane < (uint32_t)VT) {
+        const size_t col = sg.col_base + ((size_t)group * sg.g + k) * VT + lane;
+        my_partial[col] = xor4(my_partial[col], v);
+      }
+      acc[k] = make_uint4(0u, 0u, 0u, 0u);
+    }
+  };
+
+  const uint64_t i0 = gw * p.items / nw, i1 = (gw + 1) * p.items / nw;
+  for (uint64_t item = i0; item < i1; ++item) {
+    uint32_t si = 0;
+    while (si + 1 < p.nsegs && item >= p.seg[si + 1].item_begin) ++si;
+    const WarpSeg& sg = p.seg[si];
+    const uint64_t local = item - sg.item_begin;
+    const uint32_t group = (uint32_t)(local / sg.tiles);
+    const uint32_t tile = (uint32_t)(local % sg.tiles);
+    if ((int)si != cur_seg || group != cur_group) {
+      if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
+      cur_seg = (int)si;
+      cur_group = group;
+    }
+    const uint32_t g = sg.g, M = sg.M;
+    const uint32_t F = sg.d - M;
+    const uint64_t node = (uint64_t)tile * 32 + lane;
+    const bool valid = node < sg.nF;
+    const KeyDev* __restrict__ kp = p.keys + sg.key_base + (size_t)group * g;
+    for (uint32_t k = 0; k < g; ++k) {
+      const uint64_t idx = sg.fr_base + ((uint64_t)group * g + k) * sg.nF + node;
+      w_seed[(k * slots) * 32 + lane] = valid ? p.fr_seed[idx] : make_uint4(0u, 0u, 0u, 0u);
+      w_t[(k * slots) * 32 + lane] = valid ? p.fr_t[idx] : (uint8_t)0;
+    }
+    const uint4* __restrict__ tbl = sg.table;
+    const uint64_t nrows = sg.rows;
+    const uint64_t row0 = (uint64_t)tile << (M + 5);
+    const uint32_t pairs = 1u << (M - 1);
+
+    for (uint32_t pi = 0; pi < pairs; ++pi) {
+      // Rows of this step: r = 2 * (producing lane) + leaf.
+      uint4 dat[PF > 0 ? PF : 1];
+#pragma unroll
+      for (int jj = 0; jj < PF; ++jj) {
+        const uint32_t r = r0 + (uint32_t)jj * RPL;
+        const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
+        dat[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll 1
+      for (uint32_t k = 0; k < g; ++k) {
+        const KeyDev* __restrict__ K = kp + k;
+        uint4* col_seed = w_seed + (size_t)k * slots * 32 + lane;
+        uint8_t* col_t = w_t + (size_t)k * slots * 32 + lane;
+        uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
+        uint4 s = col_seed[lvl * 32];
+        uint32_t t = col_t[lvl * 32];
+        for (;; ++lvl) {
+          uint4 Lc, Rc;
+          uint32_t tl, tr;
+          expand_cw_g(s, t, K, F + lvl, Lc, tl, Rc, tr);
+          if (lvl == M - 1) {
+            w_mask[k * 64 + 2 * lane] = leaf_mask_g(Lc, tl, K);
+            w_mask[k * 64 + 2 * lane + 1] = leaf_mask_g(Rc, tr, K);
+            break;
+          }
+          col_seed[(lvl + 1) * 32] = Rc;
+          col_t[(lvl + 1) * 32] = (uint8_t)tr;
+          s = Lc;
+          t = tl;
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int jj = 0; jj < PF; ++jj) {
+        const uint32_t r = r0 + (uint32_t)jj * RPL;
+#pragma unroll
+        for (int k = 0; k < G; ++k)
+          if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat[jj], w_mask[k * 64 + r]);
+      }
+      // Remaining loads in chunks of CH (CH divides NL - PF).
+      constexpr int REST = NL - PF;
+      constexpr int CH = REST < 8 ? (REST > 0 ? REST : 1) : 8;
+      static_assert(REST % CH == 0, "load chunks must tile the step");
+#pragma unroll 1
+      for (int j0 = PF; j0 < NL; j0 += CH) {
+        uint4 more[CH];
+#pragma unroll
+        for (int jj = 0; jj < CH; ++jj) {
+          const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
+          const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
+          more[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int jj = 0; jj < CH; ++jj) {
+          const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
+#pragma unroll
+          for (int k = 0; k < G; ++k)
+            if ((uint32_t)k < g) acc[k] = xor_and(acc[k], more[jj], w_mask[k * 64 + r]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
+}
+
 // out[c] = XOR over the nparts per-CTA partial rows.  Block = cpb columns x
 // (kThreads / cpb) slices; the slices are combined in shared memory.
 __global__ void __launch_bounds__(kThreads) reduce_kernel(const uint4* __restrict__ partial,
@@ -405,6 +614,70 @@ cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t 
   const uint64_t cap = (uint64_t)sms * 8;
   if (blocks > cap) blocks = cap;
   eval_points_kernel<<<(unsigned)blocks, 128, 0, st>>>(key, idx, n, reinterpret_cast<uint4*>(out));
+  return cudaGetLastError();
+}
+
+// ---- warp-path launchers --------------------------------------------------
+
+size_t warp_smem_bytes(int G, uint32_t slots) {
+  return (size_t)kWarps * G * (64 * 16 + (size_t)slots * 32 * 17);
+}
+
+bool warp_vt_supported(uint32_t V) { return V == 1 || V == 2 || V == 4 || V == 8 || V == 16 || V == 32; }
+
+template <int G, int VT>
+static cudaError_t warp_prepare_t(size_t smem) {
+  return cudaFuncSetAttribute(scan_warp_kernel<G, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+template <int G, int VT>
+static int warp_occupancy_t(size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_warp_kernel<G, VT>, kThreads, smem) != cudaSuccess)
+    return 0;
+  return n;
+}
+template <int G, int VT>
+static cudaError_t warp_launch_t(const WarpScanParams& p, uint32_t grid, size_t smem, cudaStream_t st) {
+  scan_warp_kernel<G, VT><<<grid, kThreads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+#define MG_VT_DISPATCH(G_, VT_, FN, ...)                \
+  switch (VT_) {                                        \
+    case 1: return FN<G_, 1>(__VA_ARGS__);              \
+    case 2: return FN<G_, 2>(__VA_ARGS__);              \
+    case 4: return FN<G_, 4>(__VA_ARGS__);              \
+    case 8: return FN<G_, 8>(__VA_ARGS__);              \
+    case 16: return FN<G_, 16>(__VA_ARGS__);            \
+    case 32: return FN<G_, 32>(__VA_ARGS__);            \
+    default: break;                                     \
+  }
+
+#define MG_GVT_DISPATCH(G, VT, FN, FAIL, ...)                 \
+  switch (G) {                                                \
+    case 1: MG_VT_DISPATCH(1, VT, FN, __VA_ARGS__) break;     \
+    case 2: MG_VT_DISPATCH(2, VT, FN, __VA_ARGS__) break;     \
+    case 3: MG_VT_DISPATCH(3, VT, FN, __VA_ARGS__) break;     \
+    case 4: MG_VT_DISPATCH(4, VT, FN, __VA_ARGS__) break;     \
+    default: break;                                           \
+  }                                                           \
+  return FAIL;
+
+bool warp_g_supported(int G) { return G >= 1 && G <= 4; }
+
+cudaError_t warp_prepare(int G, uint32_t VT, size_t smem) {
+  MG_GVT_DISPATCH(G, VT, warp_prepare_t, cudaErrorInvalidValue, smem)
+}
+int warp_occupancy(int G, uint32_t VT, size_t smem) { MG_GVT_DISPATCH(G, VT, warp_occupancy_t, 0, smem) }
+cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, size_t smem,
+                             cudaStream_t st) {
+  MG_GVT_DISPATCH(G, VT, warp_launch_t, cudaErrorInvalidValue, p, grid, smem, st)
+}
+
+cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st) {
+  if (f.n_in == 0 || nkeys == 0) return cudaSuccess;
+  dim3 grid((unsigned)f.n_in, nkeys);
+  frontier_kernel<<<grid, kThreads, 0, st>>>(f);
   return cudaGetLastError();
 }
 

@@ -344,6 +344,11 @@ class Workspace:
     def set_shape(self, subtree_bits: int = 0, keys_per_cta: int = 0) -> None:
         N.check(N.lib().mg_batch_set_shape(self.handle, subtree_bits, keys_per_cta))
 
+    def set_kernel(self, kind: str = "auto") -> None:
+        """'auto', 'cta' (any row size) or 'warp' (rows of 16..512 B)."""
+        code = {"auto": N.KERNEL_AUTO, "cta": N.KERNEL_CTA, "warp": N.KERNEL_WARP}[kind]
+        N.check(N.lib().mg_batch_set_kernel(self.handle, code))
+
     def set_keys(self, tables: Sequence[GpuPageMatrix], keys: Sequence) -> None:
         if len(tables) != len(keys):
             raise ValueError("one table per key")
@@ -353,6 +358,16 @@ class Workspace:
         self._tables, self._keys = list(tables), ka
         self._share_bytes = sum(t.row_bytes for t in tables)
         self._row_bytes = [t.row_bytes for t in tables]
+
+    def autotune(self, budget_ms: int = 0) -> dict:
+        """Time candidate launch shapes for the current keys and keep the
+        fastest (also for later passes of the same workload on this scanner)."""
+        info = N.PlanInfo()
+        ms = C.c_double()
+        N.check(N.lib().mg_batch_autotune(self.handle, budget_ms, C.byref(info), C.byref(ms)))
+        out = {f: getattr(info, f) for f, _ in info._fields_}
+        out["ms"] = ms.value
+        return out
 
     def launch(self, stream: int | None = None, graph: bool = False) -> None:
         f = N.lib().mg_batch_launch_graph if graph else N.lib().mg_batch_launch

@@ -81,11 +81,12 @@ def test_shares_match_oracle(scanner, oracle_mod, row_bytes, d, nrows):
 
 @pytest.mark.parametrize("subtree_bits", [1, 3, 8, 9, 10, 12, 14, 16])
 @pytest.mark.parametrize("keys_per_cta", [1, 2, 3, 4, 8])
-def test_every_launch_shape_is_bit_exact(scanner, oracle_mod, subtree_bits, keys_per_cta):
+def test_every_cta_kernel_shape_is_bit_exact(scanner, oracle_mod, subtree_bits, keys_per_cta):
     row_bytes, d, nrows = 32, 17, 100_003
     db, rows = make_table(scanner, oracle_mod, nrows, row_bytes, seed=5)
     keys = [oracle_keypair(oracle_mod, d, (7919 * j) % nrows, seed=6, i=j)[0] for j in range(7)]
     ws = scanner.workspace()
+    ws.set_kernel("cta")
     ws.set_shape(subtree_bits, keys_per_cta)
     g = min(keys_per_cta, 7)
     g = g if g in (1, 2, 3, 4, 8) else 4
@@ -102,7 +103,27 @@ def test_every_launch_shape_is_bit_exact(scanner, oracle_mod, subtree_bits, keys
     got = ws.read()
     assert got == oracle_mod.scan_fused(keys, rows, row_bytes)
     plan = ws.plan()
-    assert plan["keys_per_cta"] == min(keys_per_cta, 7) or keys_per_cta > 7
+    assert plan["kernel"] == N.KERNEL_CTA and plan["keys_per_cta"] == g
+    ws.close()
+
+
+@pytest.mark.parametrize("warp_tile_bits", [6, 7, 9, 12, 15])
+@pytest.mark.parametrize("keys_per_item", [1, 2, 3, 4])
+@pytest.mark.parametrize("row_bytes", [16, 32, 64, 128, 256, 512])
+def test_every_warp_kernel_shape_is_bit_exact(scanner, oracle_mod, warp_tile_bits, keys_per_item, row_bytes):
+    d, nrows = 17, 70_001
+    db, rows = make_table(scanner, oracle_mod, nrows, row_bytes, seed=7)
+    keys = [oracle_keypair(oracle_mod, d, (104729 * j) % nrows, seed=8, i=j)[0] for j in range(7)]
+    ws = scanner.workspace()
+    ws.set_kernel("warp")
+    ws.set_shape(warp_tile_bits, keys_per_item)
+    ws.set_keys([db] * len(keys), keys)
+    ws.launch()
+    got = ws.read()
+    assert got == oracle_mod.scan_fused(keys, rows, row_bytes)
+    plan = ws.plan()
+    assert plan["kernel"] == N.KERNEL_WARP and plan["subtree_bits"] == warp_tile_bits
+    assert plan["keys_per_cta"] == keys_per_item
     ws.close()
 
 
@@ -246,3 +267,29 @@ def test_plain_single_query_cpu_runnable_config(scanner, oracle_mod):
     assert b.pages == oracle_mod.scan_fused([p[1] for p in pairs], host, rb)
     for j, t in enumerate(targets):
         assert xor_bytes(a.pages[j], b.pages[j]) == host[t].tobytes()
+
+
+def test_autotuner_keeps_shares_and_caches_the_shape(scanner, oracle_mod):
+    db, rows = make_table(scanner, oracle_mod, 1 << 16, 64, seed=40)
+    keys = [oracle_keypair(oracle_mod, 16, 1000 * j + 7, seed=41, i=j)[0] for j in range(3)]
+    ws = scanner.workspace()
+    ws.set_keys([db] * 3, keys)
+    best = ws.autotune(budget_ms=0)
+    assert best["ms"] > 0 and best["kernel"] in (N.KERNEL_CTA, N.KERNEL_WARP)
+    ws.launch()
+    want = oracle_mod.scan_fused(keys, rows, 64)
+    assert ws.read() == want
+    # A fresh workspace with the same workload picks the tuned shape up.
+    ws2 = scanner.workspace()
+    other = [oracle_keypair(oracle_mod, 16, 999 * j + 1, seed=42, i=j)[0] for j in range(3)]
+    ws2.set_keys([db] * 3, other)
+    plan = ws2.plan()
+    for f in ("kernel", "subtree_bits", "keys_per_cta"):
+        assert plan[f] == best[f]
+    ws2.launch()
+    assert ws2.read() == oracle_mod.scan_fused(other, rows, 64)
+    # ... and so does the one-call entry point.
+    got, _ = scanner.scan_keys(db, other)
+    assert got == oracle_mod.scan_fused(other, rows, 64)
+    ws.close()
+    ws2.close()
