@@ -146,13 +146,25 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
       }
       __syncthreads();
       if (scan_thread) {
-        for (uint32_t r = rslot; r < 2 * NR; r += rpi) {
-          const uint64_t row = tile_row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
-          if (row < nrows) {
-            const uint4 dat = __ldg(tbl + row * V + lane);
+        // Eight independent 128-bit loads in flight per thread before any
+        // is consumed (wide rows leave one lane position per thread, so
+        // this is what keeps enough bytes in flight for HBM).
+        for (uint32_t rb = rslot; rb < 2 * NR; rb += 8 * rpi) {
+          uint4 dat[8];
 #pragma unroll
-            for (int k = 0; k < G; ++k)
-              if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat, s_mask[(size_t)k * 2 * kThreads + r]);
+          for (int u = 0; u < 8; ++u) {
+            const uint32_t r = rb + (uint32_t)u * rpi;
+            const uint64_t row = tile_row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
+            dat[u] = (r < 2 * NR && row < nrows) ? __ldg(tbl + row * V + lane) : make_uint4(0u, 0u, 0u, 0u);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const uint32_t r = rb + (uint32_t)u * rpi;
+            if (r < 2 * NR) {
+#pragma unroll
+              for (int k = 0; k < G; ++k)
+                if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat[u], s_mask[(size_t)k * 2 * kThreads + r]);
+            }
           }
         }
       }

@@ -208,3 +208,52 @@ def fill_test_rows(nrows: int, row_bytes: int) -> np.ndarray:
     buf = np.zeros(nrows * row_bytes, np.uint8)
     lib().mgo_fill_test_rows(buf.ctypes.data_as(C.POINTER(C.c_uint8)), nrows, row_bytes)
     return buf
+
+
+# ---- the reference's own CUDA kernels (built by oracle/ref_build.py) -------
+
+REF_LIB_PATH = HERE / "_ref" / "libmg_refkernels.so"
+REF_MAX_DOMAIN_BITS = 25
+REF_PAGE_BYTES = 4096
+_ref = None
+
+
+def ref_available() -> bool:
+    return REF_LIB_PATH.exists()
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(str(REF_LIB_PATH))
+        L.ref_key_pod.argtypes = [C.POINTER(C.c_uint8), C.c_size_t, C.POINTER(C.c_uint8)]
+        L.ref_scan.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint8),
+                               C.POINTER(C.c_uint8), C.c_int, C.POINTER(C.c_float)]
+        _ref = L
+    return _ref
+
+
+def ref_scan(kind: int, keys, db_dev_ptr: int, num_pages: int, reps: int = 1):
+    """Run the reference kernel over num_pages 4096-byte pages at db_dev_ptr.
+    kind 0: baseline fused_batch_pir_kernel_1 (3 keys); kind 1: optimized
+    kernel with batch = len(keys) / 3 in {1, 2, 4}.  Returns (shares, best ms)."""
+    L = ref_lib()
+    nk = len(keys)
+    if nk % 3:
+        raise ValueError("the reference kernels take 3 keys per query")
+    pods = np.zeros(nk * 488, np.uint8)
+    for i, k in enumerate(keys):
+        kb = np.frombuffer(bytes(k), np.uint8)
+        if kb[18] > REF_MAX_DOMAIN_BITS:
+            raise ValueError("the reference kernel evaluates at most 25 levels")
+        rc = L.ref_key_pod(kb.ctypes.data_as(C.POINTER(C.c_uint8)), kb.size,
+                           pods[i * 488:].ctypes.data_as(C.POINTER(C.c_uint8)))
+        if rc:
+            raise ValueError("malformed key")
+    out = np.zeros(nk * REF_PAGE_BYTES, np.uint8)
+    ms = C.c_float()
+    rc = L.ref_scan(kind, nk // 3, C.c_void_p(db_dev_ptr), num_pages, pods.ctypes.data_as(C.POINTER(C.c_uint8)),
+                    out.ctypes.data_as(C.POINTER(C.c_uint8)), reps, C.byref(ms))
+    if rc:
+        raise RuntimeError(f"reference kernel launch failed (cudaError {rc})")
+    return [out[i * REF_PAGE_BYTES:(i + 1) * REF_PAGE_BYTES].tobytes() for i in range(nk)], ms.value

@@ -206,3 +206,22 @@ def test_nonbinary_t_bytes_follow_reference_semantics(oracle_mod):
     full = oracle_mod.eval_subtree(k, 0, 64)
     for i in range(64):
         assert full[i].tobytes() == oracle_mod.eval_point(k, i)
+
+
+def test_oracle_matches_reference_kernel_fixtures(oracle_mod):
+    """Shares recorded from the reference's own CUDA kernel
+    (cuda/fused_kernel.cu, fused_batch_pir_kernel_1, built for sm_100a and run
+    on a B200 by tests/golden/make_ref_fixtures.py) for make_test_pages pages
+    (kernel.rs:1390-1403): the oracle reproduces every one."""
+    import hashlib
+    data = json.loads((GOLDEN / "ref_kernel_pages.json").read_text())
+    assert len(data["cases"]) >= 4
+    for case in data["cases"]:
+        pages = oracle_mod.fill_test_rows(case["pages"], 4096)
+        keys = [bytes.fromhex(k) for k in case["keys"]]
+        got = oracle_mod.scan_fused(keys, pages, 4096)
+        for j, share in enumerate(got):
+            assert hashlib.sha256(share).hexdigest() == case["sha256"][j]
+            assert share[:64].hex() == case["head"][j] and share[-64:].hex() == case["tail"][j]
+            if "shares" in case:
+                assert share.hex() == case["shares"][j]
