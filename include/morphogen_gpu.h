@@ -104,6 +104,26 @@ int mg_table_fill_splitmix(mg_table* table, uint64_t seed);
  * the XOR patch of try_build_snapshot_from_entries, server/epoch.rs:118-181).
  * Host arrays; row indices must be < rows. */
 int mg_table_xor_rows(mg_table* table, const uint64_t* row_idx, const void* diffs, uint64_t n);
+/* ---- epoch delta: DeltaBuffer + scan_delta_for_gpu + epoch merge --------- */
+/* A table may hold a device-resident buffer of pending row updates
+ * (crates/morphogen-core/src/delta.rs: DeltaEntry{row_idx, diff}).  Every
+ * pass over the table folds the pending entries into each key's share:
+ * share ^= XOR_e diff_e & eval(row_e) (scan_delta_for_gpu,
+ * crates/morphogen-server/src/scan.rs:434-485, in row mode), so answers
+ * reflect table XOR delta without touching the table.  mg_table_delta_merge
+ * XOR-patches the table with the entries, clears the buffer and advances the
+ * epoch (the merge of EpochManager::try_advance,
+ * crates/morphogen-server/src/epoch.rs:465-549).  Merge and clear wait for
+ * every pass already enqueued on the device; the caller must not enqueue a
+ * pass over the table while they run (the reference's matrix lock). */
+int mg_table_delta_reserve(mg_table* table, uint32_t capacity);
+/* DeltaBuffer::push: append n entries (host arrays, diffs n x row_bytes).
+ * MG_ERANGE when the buffer is full or a row index is outside the table. */
+int mg_table_delta_push(mg_table* table, const uint64_t* row_idx, const void* diffs, uint32_t n);
+uint32_t mg_table_delta_count(const mg_table* table);
+int mg_table_delta_clear(mg_table* table);
+int mg_table_delta_merge(mg_table* table);
+uint64_t mg_table_epoch(const mg_table* table);
 uint64_t mg_table_rows(const mg_table* table);
 uint32_t mg_table_row_bytes(const mg_table* table);
 const void* mg_table_device_ptr(const mg_table* table);

@@ -30,7 +30,8 @@ EXPORTED = (
     "mg_context_create", "mg_context_destroy", "mg_last_error", "mg_device_info",
     "mg_table_create", "mg_table_destroy", "mg_table_write_rows", "mg_table_read_rows",
     "mg_table_fill_splitmix", "mg_table_xor_rows", "mg_table_rows", "mg_table_row_bytes",
-    "mg_table_device_ptr", "mg_key_size", "mg_key_check", "mg_keygen", "mg_scan",
+    "mg_table_device_ptr", "mg_table_delta_reserve", "mg_table_delta_push", "mg_table_delta_count",
+    "mg_table_delta_clear", "mg_table_delta_merge", "mg_table_epoch", "mg_key_size", "mg_key_check", "mg_keygen", "mg_scan",
     "mg_batch_create", "mg_batch_destroy", "mg_batch_set_keys", "mg_batch_set_shape", "mg_batch_set_kernel",
     "mg_batch_autotune",
     "mg_batch_launch", "mg_batch_launch_graph", "mg_batch_read", "mg_batch_sync",
@@ -107,6 +108,12 @@ def lib():
             "mg_table_rows": ([vp], C.c_uint64),
             "mg_table_row_bytes": ([vp], C.c_uint32),
             "mg_table_device_ptr": ([vp], vp),
+            "mg_table_delta_reserve": ([vp, C.c_uint32], C.c_int),
+            "mg_table_delta_push": ([vp, u64p, vp, C.c_uint32], C.c_int),
+            "mg_table_delta_count": ([vp], C.c_uint32),
+            "mg_table_delta_clear": ([vp], C.c_int),
+            "mg_table_delta_merge": ([vp], C.c_int),
+            "mg_table_epoch": ([vp], C.c_uint64),
             "mg_key_size": ([C.c_uint32], sz),
             "mg_key_check": ([u8p, sz, C.POINTER(C.c_uint32), u8p], C.c_int),
             "mg_keygen": ([C.c_uint32, C.c_uint64, u8p, u8p, u8p, u8p], C.c_int),

@@ -152,6 +152,14 @@ struct mg_table {
   void* d = nullptr;
   uint64_t rows = 0;
   uint32_t row_bytes = 0;
+  // Pending epoch delta (DeltaBuffer, crates/morphogen-core/src/delta.rs):
+  // entries are folded into every pass over the table until merged.
+  uint64_t* d_delta_idx = nullptr;
+  void* d_delta_diff = nullptr;
+  uint32_t* d_delta_count = nullptr;  // entry count read by the delta kernel
+  uint32_t delta_cap = 0;
+  uint32_t delta_count = 0;
+  uint64_t epoch = 0;
 };
 
 struct mg_batch {
@@ -188,6 +196,14 @@ struct mg_batch {
   uint8_t* d_tmp_t[2] = {nullptr, nullptr};
   size_t cap_tmp = 0;
   std::vector<Launch> launches;
+  struct DeltaLaunch {
+    const mg_table* table;
+    uint32_t job0, njobs;  // range in d_jobs
+  };
+  std::vector<DeltaLaunch> deltas;
+  uint2* d_jobs = nullptr;
+  uint2* h_jobs = nullptr;
+  size_t cap_jobs = 0;
   uint32_t total_cols = 0;
   std::vector<uint32_t> key_col;    // first share column of input key i
   std::vector<uint32_t> key_bytes;  // share bytes of input key i
@@ -415,6 +431,9 @@ int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table
 int mg_table_destroy(mg_table* t) {
   if (!t) return MG_OK;
   set_device(t);
+  if (t->d_delta_idx) cudaFree(t->d_delta_idx);
+  if (t->d_delta_diff) cudaFree(t->d_delta_diff);
+  if (t->d_delta_count) cudaFree(t->d_delta_count);
   if (t->d) cudaFree(t->d);
   delete t;
   return MG_OK;
@@ -480,6 +499,98 @@ int mg_table_xor_rows(mg_table* t, const uint64_t* idx, const void* diffs, uint6
 uint64_t mg_table_rows(const mg_table* t) { return t ? t->rows : 0; }
 uint32_t mg_table_row_bytes(const mg_table* t) { return t ? t->row_bytes : 0; }
 const void* mg_table_device_ptr(const mg_table* t) { return t ? t->d : nullptr; }
+
+int mg_table_delta_reserve(mg_table* t, uint32_t capacity) {
+  if (!t) return fail(MG_EINVAL, "null table");
+  if (capacity < t->delta_count)
+    return fail(MG_EINVAL, "capacity %u below the %u pending entries", capacity, t->delta_count);
+  if (capacity == t->delta_cap) return MG_OK;
+  if (int rc = set_device(t)) return rc;
+  uint64_t* idx = nullptr;
+  void* diff = nullptr;
+  uint32_t* cnt = t->d_delta_count;
+  if (capacity) {
+    if (cudaMalloc(&idx, (size_t)capacity * 8) != cudaSuccess ||
+        cudaMalloc(&diff, (size_t)capacity * t->row_bytes) != cudaSuccess ||
+        (!cnt && cudaMalloc(&cnt, 4) != cudaSuccess)) {
+      cudaGetLastError();
+      if (idx) cudaFree(idx);
+      if (diff) cudaFree(diff);
+      return fail(MG_ENOMEM, "cannot allocate a %u-entry delta buffer", capacity);
+    }
+    cudaError_t e = cudaSuccess;
+    if (t->delta_count) {
+      e = cudaMemcpy(idx, t->d_delta_idx, (size_t)t->delta_count * 8, cudaMemcpyDeviceToDevice);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(diff, t->d_delta_diff, (size_t)t->delta_count * t->row_bytes, cudaMemcpyDeviceToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(cnt, &t->delta_count, 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(idx);
+      cudaFree(diff);
+      return fail(MG_ECUDA, "delta reserve: %s", cudaGetErrorString(e));
+    }
+  }
+  if (t->d_delta_idx) cudaFree(t->d_delta_idx);
+  if (t->d_delta_diff) cudaFree(t->d_delta_diff);
+  t->d_delta_idx = idx;
+  t->d_delta_diff = diff;
+  t->d_delta_count = cnt;
+  t->delta_cap = capacity;
+  return MG_OK;
+}
+
+int mg_table_delta_push(mg_table* t, const uint64_t* row_idx, const void* diffs, uint32_t n) {
+  if (!t || (n && (!row_idx || !diffs))) return fail(MG_EINVAL, "null argument");
+  if (n == 0) return MG_OK;
+  if ((uint64_t)t->delta_count + n > t->delta_cap)
+    return fail(MG_ERANGE, "delta buffer full: %u entries (max %u)", t->delta_count + n, t->delta_cap);
+  for (uint32_t i = 0; i < n; ++i)
+    if (row_idx[i] >= t->rows)
+      return fail(MG_ERANGE, "delta row %llu outside the %llu-row table", (unsigned long long)row_idx[i],
+                  (unsigned long long)t->rows);
+  if (int rc = set_device(t)) return rc;
+  // Entries first, then the device-side count that makes them visible.
+  MG_CUDA(cudaMemcpy(t->d_delta_idx + t->delta_count, row_idx, (size_t)n * 8, cudaMemcpyHostToDevice));
+  MG_CUDA(cudaMemcpy((uint8_t*)t->d_delta_diff + (size_t)t->delta_count * t->row_bytes, diffs,
+                     (size_t)n * t->row_bytes, cudaMemcpyHostToDevice));
+  const uint32_t c = t->delta_count + n;
+  MG_CUDA(cudaMemcpy(t->d_delta_count, &c, 4, cudaMemcpyHostToDevice));
+  t->delta_count = c;
+  return MG_OK;
+}
+
+uint32_t mg_table_delta_count(const mg_table* t) { return t ? t->delta_count : 0; }
+
+int mg_table_delta_clear(mg_table* t) {
+  if (!t) return fail(MG_EINVAL, "null table");
+  if (!t->delta_cap) return MG_OK;
+  if (int rc = set_device(t)) return rc;
+  const uint32_t z = 0;
+  MG_CUDA(cudaDeviceSynchronize());
+  MG_CUDA(cudaMemcpy(t->d_delta_count, &z, 4, cudaMemcpyHostToDevice));
+  t->delta_count = 0;
+  return MG_OK;
+}
+
+int mg_table_delta_merge(mg_table* t) {
+  if (!t) return fail(MG_EINVAL, "null table");
+  if (int rc = set_device(t)) return rc;
+  // Passes already enqueued must finish against the old epoch first.
+  MG_CUDA(cudaDeviceSynchronize());
+  if (t->delta_count) {
+    MG_CUDA(mg::launch_xor_rows(t->d, t->row_bytes / 16, t->d_delta_idx, t->d_delta_diff, t->delta_count, t->sms,
+                                nullptr));
+    const uint32_t z = 0;
+    MG_CUDA(cudaMemcpy(t->d_delta_count, &z, 4, cudaMemcpyHostToDevice));
+    MG_CUDA(cudaDeviceSynchronize());
+    t->delta_count = 0;
+  }
+  ++t->epoch;
+  return MG_OK;
+}
+
+uint64_t mg_table_epoch(const mg_table* t) { return t ? t->epoch : 0; }
 
 // ---- keys -------------------------------------------------------------------
 
@@ -579,6 +690,8 @@ int mg_batch_destroy(mg_batch* b) {
   if (b->d_partial) cudaFree(b->d_partial);
   if (b->d_out) cudaFree(b->d_out);
   if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->d_jobs) cudaFree(b->d_jobs);
+  if (b->h_jobs) cudaFreeHost(b->h_jobs);
   if (b->d_fr_seed) cudaFree(b->d_fr_seed);
   if (b->d_fr_t) cudaFree(b->d_fr_t);
   for (int i = 0; i < 2; ++i) {
@@ -814,6 +927,9 @@ static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
     if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
     MG_CUDA(mg::launch_reduce(b->d_partial, L.nparts, L.cols, b->d_out + L.col0, st));
   }
+  for (const mg_batch::DeltaLaunch& dl : b->deltas)
+    MG_CUDA(mg::launch_delta(b->d_keys, b->d_jobs + dl.job0, dl.njobs, dl.table->d_delta_idx, dl.table->d_delta_diff,
+                             dl.table->d_delta_count, dl.table->delta_cap, dl.table->row_bytes / 16, b->d_out, st));
   return MG_OK;
 }
 
@@ -901,6 +1017,43 @@ int plan_pass(mg_batch* b) {
     }
   }
 
+  // Delta folding: one launch per table that holds a delta buffer.
+  std::vector<mg_batch::DeltaLaunch> deltas;
+  std::vector<uint2> jobs;
+  for (uint32_t i = 0; i < nkeys; ++i) {
+    const mg_table* t = b->in_tables[i];
+    if (!t->delta_cap) continue;
+    auto it = std::find_if(deltas.begin(), deltas.end(), [&](const mg_batch::DeltaLaunch& x) { return x.table == t; });
+    if (it == deltas.end()) {
+      deltas.push_back({t, 0, 0});
+      it = deltas.end() - 1;
+    }
+  }
+  for (mg_batch::DeltaLaunch& dl : deltas) {
+    dl.job0 = (uint32_t)jobs.size();
+    for (uint32_t i = 0; i < nkeys; ++i)
+      if (b->in_tables[i] == dl.table) jobs.push_back(make_uint2(key_slot[i], key_col[i]));
+    dl.njobs = (uint32_t)jobs.size() - dl.job0;
+  }
+  if (jobs.size() > b->cap_jobs) {
+    if (b->d_jobs) cudaFree(b->d_jobs);
+    if (b->h_jobs) cudaFreeHost(b->h_jobs);
+    b->d_jobs = nullptr;
+    b->h_jobs = nullptr;
+    b->cap_jobs = 0;
+    if (cudaMalloc(&b->d_jobs, jobs.size() * sizeof(uint2)) != cudaSuccess ||
+        cudaMallocHost(&b->h_jobs, jobs.size() * sizeof(uint2)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MG_ENOMEM, "cannot allocate delta job lists");
+    }
+    b->cap_jobs = jobs.size();
+  }
+  if (!jobs.empty()) {
+    std::memcpy(b->h_jobs, jobs.data(), jobs.size() * sizeof(uint2));
+    MG_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, jobs.size() * sizeof(uint2), cudaMemcpyHostToDevice, b->stream));
+  }
+  b->deltas = std::move(deltas);
+
   size_t max_partial = 0;
   for (const mg_batch::Launch& L : launches) max_partial = std::max(max_partial, (size_t)L.nparts * L.cols);
   if (int rc = grow(b, nkeys, max_partial, total_cols, (size_t)fr_cursor, tmp_need)) return rc;
@@ -957,6 +1110,7 @@ int plan_pass(mg_batch* b) {
   b->info.frontier_nodes = (uint32_t)std::min<uint64_t>(fr_cursor, 0xFFFFFFFFu);
   b->info.kernels = 0;
   for (const mg_batch::Launch& L : b->launches) b->info.kernels += 2 + (uint32_t)L.steps.size();
+  b->info.kernels += (uint32_t)b->deltas.size();
   b->planned = true;
   return MG_OK;
 }
@@ -1151,6 +1305,11 @@ int mg_batch_launch_graph(mg_batch* b, void* stream) {
     if (L.kind == MG_KERNEL_CTA) add(&L.p, sizeof L.p);
     else add(&L.w, sizeof L.w);
     for (const mg::FrontierStep& f : L.steps) add(&f, sizeof f);
+  }
+  for (const mg_batch::DeltaLaunch& dl : b->deltas) {
+    add(&dl, sizeof dl);
+    add(&dl.table->d_delta_idx, sizeof dl.table->d_delta_idx);
+    add(&dl.table->delta_cap, sizeof dl.table->delta_cap);
   }
   const uint8_t* op = reinterpret_cast<const uint8_t*>(&b->d_out);
   sig.insert(sig.end(), op, op + sizeof b->d_out);

@@ -31,6 +31,10 @@ int warp_occupancy(int G, uint32_t VT, size_t smem);
 cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, size_t smem,
                              cudaStream_t st);
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st);
+// Folds a table's pending delta into the shares: jobs[j] = (key slot, first share column).
+cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, const uint64_t* idx,
+                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint4* out,
+                         cudaStream_t st);
 
 // Sets the thread-local message returned by mg_last_error().
 void set_last_error(const char* msg);

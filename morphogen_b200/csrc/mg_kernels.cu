@@ -20,6 +20,7 @@
 // schedule.  The kernels contain no waits on other CTAs or on the host.
 #include "mg_device.cuh"
 #include "mg_internal.h"
+#include "morphogen_gpu.h"
 
 namespace mg {
 
@@ -441,6 +442,77 @@ __global__ void __launch_bounds__(kThreads) reduce_kernel(const uint4* __restric
   }
 }
 
+// ChaChaKey::eval (dpf.rs:103-142) of one index: the d-level path walk.
+__device__ __forceinline__ uint4 eval_leaf(const KeyDev* __restrict__ K, uint64_t x) {
+  uint4 s = __ldg(&K->root_seed);
+  uint32_t t = __ldg(&K->root_t);
+  const uint32_t d = __ldg(&K->domain_bits);
+  for (uint32_t lvl = 0; lvl < d; ++lvl) {
+    uint4 Lc, Rc;
+    uint32_t tl, tr;
+    expand_cw_g(s, t, K, lvl, Lc, tl, Rc, tr);
+    const uint32_t bit = (uint32_t)(x >> (d - 1 - lvl)) & 1u;
+    s = bit ? Rc : Lc;
+    t = bit ? tr : tl;
+  }
+  return leaf_mask_g(s, t, K);
+}
+
+// Pending epoch delta of a table folded into the shares of the pass
+// (scan_delta_for_gpu, crates/morphogen-server/src/scan.rs:434-485, in row
+// mode): out[col_j] ^= XOR_e diff_e & eval_j(row_e) for every job j (a key
+// scanned over this table).  One thread per entry evaluates its row; each
+// 16-byte position is XOR-reduced across the warp with shuffles, then across
+// the CTA in shared memory, and the CTA's result is XORed into the share
+// with one atomic per word (XOR is order-independent, so the result is
+// deterministic).  The entry count is read on the device so that pushes are
+// seen by replayed graphs.
+__global__ void __launch_bounds__(kThreads) delta_kernel(const KeyDev* __restrict__ keys, const uint2* __restrict__ jobs,
+                                                         const uint64_t* __restrict__ idx, const uint4* __restrict__ diffs,
+                                                         const uint32_t* __restrict__ count, uint32_t V,
+                                                         uint4* __restrict__ out) {
+  __shared__ uint4 s_acc[MG_MAX_ROW_BYTES / 16];
+  const uint32_t n = *count;
+  const uint64_t e0 = (uint64_t)blockIdx.x * kThreads;
+  if (e0 >= n) return;  // uniform per CTA
+  const uint2 job = jobs[blockIdx.y];
+  const KeyDev* __restrict__ K = keys + job.x;
+  for (uint32_t v = threadIdx.x; v < V; v += kThreads) s_acc[v] = make_uint4(0u, 0u, 0u, 0u);
+  const uint64_t e = e0 + threadIdx.x;
+  const bool live = e < n;
+  const uint4 m = live ? eval_leaf(K, idx[e]) : make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t v = 0; v < V; ++v) {
+    uint4 c = live ? diffs[e * V + v] : make_uint4(0u, 0u, 0u, 0u);
+    c.x &= m.x; c.y &= m.y; c.z &= m.z; c.w &= m.w;
+#pragma unroll
+    for (uint32_t off = 16; off >= 1; off >>= 1) {
+      c.x ^= __shfl_xor_sync(0xFFFFFFFFu, c.x, off);
+      c.y ^= __shfl_xor_sync(0xFFFFFFFFu, c.y, off);
+      c.z ^= __shfl_xor_sync(0xFFFFFFFFu, c.z, off);
+      c.w ^= __shfl_xor_sync(0xFFFFFFFFu, c.w, off);
+    }
+    if (lane == 0 && (c.x | c.y | c.z | c.w)) {
+      atomicXor(&s_acc[v].x, c.x);
+      atomicXor(&s_acc[v].y, c.y);
+      atomicXor(&s_acc[v].z, c.z);
+      atomicXor(&s_acc[v].w, c.w);
+    }
+  }
+  __syncthreads();
+  for (uint32_t v = threadIdx.x; v < V; v += kThreads) {
+    const uint4 a = s_acc[v];
+    if (a.x | a.y | a.z | a.w) {
+      unsigned int* o = reinterpret_cast<unsigned int*>(out + job.y + v);
+      atomicXor(o + 0, a.x);
+      atomicXor(o + 1, a.y);
+      atomicXor(o + 2, a.z);
+      atomicXor(o + 3, a.w);
+    }
+  }
+}
+
 // SplitMix64 output `w` of the stream seeded with `seed` (Steele, Lea, Flood 2014).
 __device__ __forceinline__ uint64_t splitmix_word(uint64_t seed, uint64_t w) {
   uint64_t z = seed + (w + 1) * 0x9E3779B97F4A7C15ull;
@@ -684,6 +756,15 @@ int warp_occupancy(int G, uint32_t VT, size_t smem) { MG_GVT_DISPATCH(G, VT, war
 cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, size_t smem,
                              cudaStream_t st) {
   MG_GVT_DISPATCH(G, VT, warp_launch_t, cudaErrorInvalidValue, p, grid, smem, st)
+}
+
+cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, const uint64_t* idx,
+                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint4* out,
+                         cudaStream_t st) {
+  if (njobs == 0 || capacity == 0) return cudaSuccess;
+  dim3 grid((capacity + kThreads - 1) / kThreads, njobs);
+  delta_kernel<<<grid, kThreads, 0, st>>>(keys, jobs, idx, reinterpret_cast<const uint4*>(diffs), count, V, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st) {

@@ -304,6 +304,30 @@ class GpuPageMatrix:
         N.check(N.lib().mg_table_xor_rows(self.handle, idx.ctypes.data_as(C.POINTER(C.c_uint64)),
                                           d.ctypes.data_as(C.c_void_p), idx.size))
 
+    # -- epoch delta (DeltaBuffer / scan_delta_for_gpu / epoch merge) -------
+    def delta_reserve(self, capacity: int) -> None:
+        N.check(N.lib().mg_table_delta_reserve(self.handle, capacity))
+
+    def delta_push(self, row_idx, diffs) -> None:
+        idx = np.ascontiguousarray(row_idx, dtype=np.uint64)
+        d = np.ascontiguousarray(diffs, dtype=np.uint8).reshape(-1)
+        if d.size != idx.size * self.row_bytes:
+            raise ValueError("diffs must hold one row per index")
+        N.check(N.lib().mg_table_delta_push(self.handle, idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                            d.ctypes.data_as(C.c_void_p), idx.size))
+
+    def delta_count(self) -> int:
+        return int(N.lib().mg_table_delta_count(self.handle))
+
+    def delta_clear(self) -> None:
+        N.check(N.lib().mg_table_delta_clear(self.handle))
+
+    def delta_merge(self) -> None:
+        N.check(N.lib().mg_table_delta_merge(self.handle))
+
+    def epoch(self) -> int:
+        return int(N.lib().mg_table_epoch(self.handle))
+
     def num_pages(self) -> int:
         return self._rows
 
