@@ -46,6 +46,9 @@ WORKLOADS = {
                     rows=1 << 20, row_bytes=256, d=20),
     "batched31": dict(name="batched queries per pass, 2^31 rows x 32 B (64 GiB), 31-bit keys",
                       rows=1 << 31, row_bytes=32, d=31),
+    "serve31": dict(name="serving loop over 2^31 rows x 32 B (64 GiB): Poisson arrivals, 1-32 lookups per "
+                         "request (geometric, mean 4), 3 x 31-bit keys per lookup, 2^16-row epoch delta "
+                         "replaced and merged every 12 s", rows=1 << 31, row_bytes=32, d=31),
 }
 KEYS_PER_QUERY = 3
 SEED = 0
@@ -171,6 +174,80 @@ def run_reference(args, rank: int, world: int):
         "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                          "sample": desc + "; ms_per_step extrapolates to the full table"},
         "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, local_rank: int):
+    """Continuous-batching serving loop at several Poisson arrival rates."""
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+    from morphogen_b200.server import PirServer, geometric_lookups, poisson_load
+
+    torch.cuda.set_device(local_rank)
+    wl = WORKLOADS["serve31"]
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    scanner = G.GpuScanner(local_rank)
+    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
+    drng = np.random.default_rng(SEED + 1)
+    delta_rows = 1 << 16
+    table.delta_reserve(delta_rows)
+
+    def new_delta():
+        idx = drng.integers(0, rows, delta_rows).astype(np.uint64)
+        diffs = drng.integers(0, 256, delta_rows * rb, dtype=np.uint8)
+        table.delta_push(idx, diffs)
+
+    new_delta()
+    pool, _, _ = seeded_keys(d, rows, 64)  # 64 lookups x 3 keys
+    lookups = [pool[3 * i:3 * i + 3] for i in range(64)]
+
+    def make_request(rng):
+        n = geometric_lookups(rng, mean=4.0, lo=1, hi=32)
+        items = []
+        for _ in range(n):
+            items += [(table, k) for k in lookups[int(rng.integers(0, len(lookups)))]]
+        return items
+
+    srv = PirServer(scanner, slots=2)
+    # Single-lookup latency with an idle server (the plain path through the loop).
+    for _ in range(2):
+        srv.answer(make_request(np.random.default_rng(0))[:3])
+    srv.reset_stats()
+    for _ in range(5):
+        srv.answer([(table, k) for k in lookups[0]])
+    idle = srv.stats()
+    merges = {"count": 0, "next": 12.0}
+
+    def tick(t):
+        if t >= merges["next"]:
+            srv.pause()
+            table.delta_merge()
+            new_delta()
+            srv.resume()
+            merges["count"] += 1
+            merges["next"] += 12.0
+
+    points = []
+    rates = [float(x) for x in args.rates.split(",")]
+    for rate in rates:
+        merges["next"] = 12.0
+        dur = args.duration if rate <= 5 else args.overload_duration
+        st = poisson_load(srv, make_request, rate, dur, seed=int(rate * 1000), tick=tick)
+        points.append({"offered_req_per_s": round(st["offered_req_per_s"], 3), "requests": st["requests"],
+                       "lookups": st["keys"] // 3, "answered_lookups_per_s": round(st["answered_keys_per_s"] / 3, 3),
+                       "p50_ms": round(st["p50_ms"], 1), "p95_ms": round(st["p95_ms"], 1),
+                       "p99_ms": round(st["p99_ms"], 1), "passes": st["passes"], "failed": st["failed"]})
+    srv.close()
+    best = max(p["answered_lookups_per_s"] for p in points)
+    line = {
+        "metric": "answered lookups/s (3 keys each) and p50/p95/p99 latency under Poisson load",
+        "value": best, "unit": "lookups/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
+        "data": "synthetic", "config": {"workload": wl["name"], "slots": 2, "delta_rows": delta_rows,
+                                        "merge_interval_s": 12, "epoch_merges": merges["count"]},
+        "idle_single_lookup_ms": {"p50": round(idle["p50_ms"], 2), "p99": round(idle["p99_ms"], 2)},
+        "load_points": points,
     }
     print(json.dumps(line), flush=True)
 
@@ -342,6 +419,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--autotune", type=int, default=-1,
                     help="autotuner budget in ms before timing (-1: 5000 when a pass is under 20 ms, else off)")
+    ap.add_argument("--rates", default="0.25,0.5,1,2,100",
+                    help="serve31: Poisson arrival rates (requests/s) to run")
+    ap.add_argument("--duration", type=float, default=20.0, help="serve31: seconds of arrivals per rate")
+    ap.add_argument("--overload-duration", type=float, default=1.0,
+                    help="serve31: seconds of arrivals for rates above capacity")
     ap.add_argument("--kernel", default="auto", choices=["auto", "cta", "warp"],
                     help="scan kernel for the device-resident passes (default: the planner's choice)")
     args = ap.parse_args()
@@ -352,6 +434,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "serve31":
+        if rank == 0:
+            run_serve(args, local_rank)
     else:
         run_gpu(args, rank, world, local_rank)
 

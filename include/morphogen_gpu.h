@@ -196,6 +196,48 @@ int mg_prg_peak(mg_context* ctx, uint32_t iters, double* expands_per_s);
 int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const uint64_t* idx,
                    uint64_t n, uint8_t* out);
 
+/* ---- serving loop: continuous batching (network/api/mod.rs:544-838) ------- */
+/* A dispatcher thread owns `slots` workspaces (one stream each).  Whenever
+ * one is free it folds every request that has arrived into one pass, so
+ * requests that arrive while others are on the GPU join the next pass and
+ * passes of different workspaces overlap on the device.  A request is
+ * admitted when the device memory its keys, frontier and partial rows need
+ * fits in free memory minus memory_reserve (or when nothing else runs).
+ * Tables and their delta buffers stay resident; for an epoch merge call
+ * mg_server_pause (drains in-flight passes), mg_table_delta_merge, then
+ * mg_server_resume. */
+typedef struct {
+  uint32_t slots;             /* concurrent passes (default 2) */
+  uint32_t max_keys_per_pass; /* 0 = no cap */
+  uint64_t memory_reserve;    /* device bytes kept free (default 1 GiB) */
+} mg_server_config;
+
+typedef struct {
+  uint64_t completed;       /* requests answered */
+  uint64_t failed;
+  uint64_t passes;
+  uint64_t keys_completed;  /* keys (DPF evaluations) answered */
+  uint32_t pending;         /* requests waiting for a pass */
+  uint32_t in_flight;       /* passes on the GPU */
+  double wall_s;            /* since create / reset */
+  double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;  /* submit -> answered */
+} mg_server_stats;
+
+typedef struct mg_server mg_server;
+int mg_server_create(mg_context* ctx, const mg_server_config* cfg, mg_server** out);
+int mg_server_destroy(mg_server* server);
+/* Queue one request (its keys, key i over tables[i]); returns its id. */
+int mg_server_submit(mg_server* server, const mg_table* const* tables, const uint8_t* const* keys,
+                     const size_t* key_lens, uint32_t nkeys, uint64_t* request_id);
+/* Wait for a request (0 = no deadline) and copy its shares (back to back).
+ * The id is released on return, except on MG_ETIMEDOUT. */
+int mg_server_wait(mg_server* server, uint64_t request_id, uint8_t* out_shares, uint32_t timeout_ms,
+                   double* latency_ms);
+int mg_server_pause(mg_server* server, uint32_t timeout_ms);
+int mg_server_resume(mg_server* server);
+int mg_server_get_stats(mg_server* server, mg_server_stats* stats);
+int mg_server_reset_stats(mg_server* server);
+
 /* ---- allocation-free scan (no counterpart in the reference) -------------- */
 /* For callers that cannot call cudaMalloc: the host application or a memory
  * pool owns all device memory (plugins, embedded servers), or cudaMalloc /

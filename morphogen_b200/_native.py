@@ -37,6 +37,8 @@ EXPORTED = (
     "mg_batch_launch", "mg_batch_launch_graph", "mg_batch_read", "mg_batch_sync",
     "mg_batch_shares_device", "mg_batch_plan", "mg_batch_last_kernel_ns", "mg_batch_last_scan_ns",
     "mg_eval_points", "mg_prg_peak", "mg_scan_noalloc",
+    "mg_server_create", "mg_server_destroy", "mg_server_submit", "mg_server_wait", "mg_server_pause",
+    "mg_server_resume", "mg_server_get_stats", "mg_server_reset_stats",
 )
 
 
@@ -73,6 +75,17 @@ class PlanInfo(C.Structure):
 
 
 KERNEL_AUTO, KERNEL_CTA, KERNEL_WARP = 0, 1, 2
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("max_keys_per_pass", C.c_uint32), ("memory_reserve", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("passes", C.c_uint64),
+                ("keys_completed", C.c_uint64), ("pending", C.c_uint32), ("in_flight", C.c_uint32),
+                ("wall_s", C.c_double), ("p50_ms", C.c_double), ("p95_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_ms", C.c_double), ("max_ms", C.c_double)]
 
 
 _lib = None
@@ -135,6 +148,14 @@ def lib():
             "mg_batch_last_scan_ns": ([vp, u64p], C.c_int),
             "mg_prg_peak": ([vp, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
             "mg_eval_points": ([vp, u8p, sz, u64p, C.c_uint64, u8p], C.c_int),
+            "mg_server_create": ([vp, C.POINTER(ServerConfig), C.POINTER(vp)], C.c_int),
+            "mg_server_destroy": ([vp], C.c_int),
+            "mg_server_submit": ([vp, C.POINTER(vp), C.POINTER(u8p), C.POINTER(sz), C.c_uint32, u64p], C.c_int),
+            "mg_server_wait": ([vp, C.c_uint64, u8p, C.c_uint32, C.POINTER(C.c_double)], C.c_int),
+            "mg_server_pause": ([vp, C.c_uint32], C.c_int),
+            "mg_server_resume": ([vp], C.c_int),
+            "mg_server_get_stats": ([vp, C.POINTER(ServerStats)], C.c_int),
+            "mg_server_reset_stats": ([vp], C.c_int),
             "mg_scan_noalloc": ([C.c_int, vp, C.c_uint64, C.c_uint32, C.POINTER(u8p), C.POINTER(sz),
                                  C.c_uint32, vp, vp], C.c_int),
         }

@@ -16,7 +16,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libmorphogen_gpu.so"
-SOURCES = [CSRC / "mg_kernels.cu", CSRC / "mg_api.cu", CSRC / "mg_noalloc.cu"]
+SOURCES = [CSRC / "mg_kernels.cu", CSRC / "mg_api.cu", CSRC / "mg_server.cu", CSRC / "mg_noalloc.cu"]
 HEADERS = [CSRC / "mg_device.cuh", CSRC / "mg_internal.h", ROOT / "include" / "morphogen_gpu.h"]
 
 NVCC_FLAGS = [

@@ -1521,3 +1521,15 @@ int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const ui
 }
 
 }  // extern "C"
+
+namespace mg {
+bool batch_done(mg_batch* b) {
+  if (!b->launched) return true;
+  cudaSetDevice(b->device);
+  const cudaError_t e = cudaEventQuery(b->ev_done);
+  if (e == cudaErrorNotReady) return false;
+  cudaGetLastError();
+  return true;
+}
+int context_device(const mg_context* ctx) { return ctx->device; }
+}  // namespace mg

@@ -36,6 +36,17 @@ cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, 
                          const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint4* out,
                          cudaStream_t st);
 
+}  // namespace mg
+
+struct mg_batch;
+struct mg_context;
+
+namespace mg {
+
+// True once the workspace's last enqueued work has completed on the device.
+bool batch_done(mg_batch* b);
+int context_device(const mg_context* ctx);
+
 // Sets the thread-local message returned by mg_last_error().
 void set_last_error(const char* msg);
 
