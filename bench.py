@@ -355,8 +355,19 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         e2e_per = float(tt.item())
     e2e_value = world * bytes_pass / (e2e_per * 1e-3) / 1e9
 
-    # Rooflines of the dominant kernel.
+    # Rooflines of the dominant kernel.  DRAM traffic per launch: the ratio
+    # measured by ncu on a smaller capture of the same kernel, scaled to the
+    # table bytes of this launch.
     peaks = measured_peaks()
+    traffic = None
+    try:
+        tr = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+        kname = "scan_warp_kernel" if plan.get("kernel") == 2 else "scan_kernel"
+        rec = tr.get(kname, {})
+        if rec.get("table_bytes"):
+            traffic = round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_pass)
+    except (OSError, ValueError):
+        traffic = None
     scan_avg_s = sum(scan_ns) / len(scan_ns) * 1e-9
     achieved_hbm = bytes_pass / scan_avg_s / 1e9
     hbm_peak = float(peaks["hbm_gbs"])
@@ -392,7 +403,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
         "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved_hbm / hbm_peak, 4), "traffic": None,
+                     "frac": round(achieved_hbm / hbm_peak, 4), "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
                      if "fallback" not in peaks else "fallback 6650 GB/s"},
         "alu": {"bound": "int32 issue (ChaCha8)", "achieved": round(achieved_nodes / 1e9, 3),

@@ -820,8 +820,16 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
     const int occ = mg::warp_occupancy(G, VT, smem);
     if (occ <= 0) continue;
     const uint64_t nw = (uint64_t)occ * ctx->sms * mg::kWarps;
-    const uint64_t per = (items + nw - 1) / nw;
-    const double bal = per ? (double)items / ((double)per * (double)nw) : 1.0;
+    // Most loaded warp under the kernel's assignment (tile-strided per
+    // segment when the key groups fit the warps, contiguous otherwise).
+    uint64_t worst = 0;
+    for (const SegPlan& sp : segs) {
+      const uint32_t M = std::min(Mt, sp.d);
+      const uint64_t tiles = (ceil_shift(sp.table->rows, M) + 31) / 32;
+      const uint64_t groups = sp.keys.size() / sp.g;
+      worst += (nw >= groups) ? (tiles + (nw / groups) - 1) / (nw / groups) : (groups * tiles + nw - 1) / nw;
+    }
+    const double bal = worst ? (double)items / ((double)worst * (double)nw) : 1.0;
     cands.push_back({Mt, bal, items, occ, smem});
   }
   if (cands.empty()) return fail(MG_EINVAL, "no warp-kernel shape fits the device (G=%d)", G);

@@ -260,11 +260,10 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
   }
 }
 
-// Warp-independent fused expansion + scan.  Every warp takes a contiguous
-// range of (group, warp tile) items in group-major order, so consecutive
-// items usually belong to the same keys and the accumulators stay in
-// registers; they are flushed (warp shuffle XOR) into the warp's own
-// partial row when the group changes.  Per item each lane loads its
+// Warp-independent fused expansion + scan.  Every warp keeps the same key
+// group over consecutive items (see the assignment below), so the
+// accumulators stay in registers; they are flushed (warp shuffle XOR) into
+// the warp's own partial row when the group or segment changes.  Per item each lane loads its
 // frontier node and walks its 2^M leaves depth-first (stack in the warp's
 // shared-memory slice); a step yields one leaf pair per lane for every key,
 // exchanged through shared memory with __syncwarp only, and the warp scans
@@ -325,14 +324,34 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
     }
   };
 
-  const uint64_t i0 = gw * p.items / nw, i1 = (gw + 1) * p.items / nw;
-  for (uint64_t item = i0; item < i1; ++item) {
-    uint32_t si = 0;
-    while (si + 1 < p.nsegs && item >= p.seg[si + 1].item_begin) ++si;
+  // Work assignment, per segment.  With at most as many key groups as warps,
+  // warp gw takes group gw % groups and the tiles gw / groups + k * (W /
+  // groups), W the largest multiple of groups not above the warp count: the
+  // warp keeps one key group (accumulators stay in registers) while the
+  // groups of one tile run on neighbouring warps at the same time, so a
+  // row's later reads hit L2.  With more groups than warps, each warp takes
+  // a contiguous group-major range of items.
+  for (uint32_t si = 0; si < p.nsegs; ++si) {
     const WarpSeg& sg = p.seg[si];
-    const uint64_t local = item - sg.item_begin;
-    const uint32_t group = (uint32_t)(local / sg.tiles);
-    const uint32_t tile = (uint32_t)(local % sg.tiles);
+    const uint64_t groups = sg.groups, tiles = sg.tiles;
+    const uint64_t items_s = groups * tiles;
+    const uint64_t Ws = (nw / groups) * groups;
+    uint64_t it = 0, it_end = 0, stride = 0, first_tile = 0, tile_step = 0;
+    if (Ws) {
+      if (gw >= Ws) continue;
+      first_tile = gw / groups;
+      tile_step = Ws / groups;
+      it = first_tile;
+      it_end = tiles;
+      stride = tile_step;
+    } else {
+      it = gw * items_s / nw;
+      it_end = (gw + 1) * items_s / nw;
+      stride = 1;
+    }
+    for (; it < it_end; it += stride) {
+    const uint32_t group = (uint32_t)(Ws ? gw % groups : it / tiles);
+    const uint32_t tile = (uint32_t)(Ws ? it : it % tiles);
     if ((int)si != cur_seg || group != cur_group) {
       if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
       cur_seg = (int)si;
@@ -415,6 +434,7 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
         }
       }
       __syncwarp();
+    }
     }
   }
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);

@@ -43,14 +43,28 @@ def test_each_result_is_the_same_alone_and_in_the_mix(scanner, oracle_mod, table
     reqs = make_requests(oracle_mod, tables, 16, seed=1)
     srv = PirServer(scanner, slots=2)
     alone = [srv.answer(items) for items in reqs]
-    st_alone = srv.stats()
+    assert srv.stats()["passes"] == len(reqs)
+    # Mix 1: everything arrives while dispatch is held, then is folded into
+    # as few passes as the workspaces allow.
     srv.reset_stats()
-    ids = [srv.submit(items) for items in reqs]  # all in flight together
+    srv.pause()
+    ids = [srv.submit(items) for items in reqs]
+    srv.resume()
     mixed = [srv.wait(i)[0] for i in ids]
-    st_mix = srv.stats()
+    st = srv.stats()
     assert mixed == alone
-    assert st_alone["passes"] == len(reqs)
-    assert st_mix["completed"] == len(reqs) and st_mix["passes"] < len(reqs)  # requests shared passes
+    assert st["completed"] == len(reqs) and st["passes"] <= 2
+    srv.close()
+    # Mix 2: a cap of 12 keys per pass splits the same requests into several
+    # passes that overlap on the two workspaces' streams.
+    srv = PirServer(scanner, slots=2, max_keys_per_pass=12)
+    srv.pause()
+    ids = [srv.submit(items) for items in reqs]
+    srv.resume()
+    mixed2 = [srv.wait(i)[0] for i in ids]
+    st2 = srv.stats()
+    assert mixed2 == alone
+    assert 2 < st2["passes"] < len(reqs)
     # and both equal the oracle
     for items, shares in zip(reqs[:4], alone):
         for (t, k), s in zip(items, shares):
