@@ -46,6 +46,7 @@ WORKLOADS = {
                     rows=1 << 20, row_bytes=256, d=20),
     "batched31": dict(name="batched queries per pass, 2^31 rows x 32 B (64 GiB), 31-bit keys",
                       rows=1 << 31, row_bytes=32, d=31),
+    "mixed": dict(name="accounts 2^28 x 64 B + storage 2^31 x 32 B in one pass", rows=0, row_bytes=0, d=0),
     "serve31": dict(name="serving loop over 2^31 rows x 32 B (64 GiB): Poisson arrivals, 1-32 lookups per "
                          "request (geometric, mean 4), 3 x 31-bit keys per lookup, 2^16-row epoch delta "
                          "replaced and merged every 12 s", rows=1 << 31, row_bytes=32, d=31),
@@ -156,8 +157,10 @@ def run_reference(args, rank: int, world: int):
     """The reference's CPU implementation of the path (oracle port) on the host cores."""
     if rank != 0:
         return
+    if args.workload in ("mixed", "serve31"):
+        args.workload = "plain31"
     wl = WORKLOADS[args.workload]
-    nq = args.queries if args.workload == "batched31" else 1
+    nq = int(str(args.queries).split(",")[0]) if args.workload == "batched31" else 1
     k0, _, _ = seeded_keys(wl["d"], wl["rows"], nq)
     sample = min(REF_SAMPLE_ROWS, wl["rows"])
     _, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.warmup)
@@ -252,40 +255,23 @@ def run_serve(args, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
-def run_gpu(args, rank: int, world: int, local_rank: int):
+def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist, cpu_rows=None):
+    """One workload point: correctness gate, optional autotune, K timed device
+    passes (CUDA events on the launching stream), e2e passes through mg_scan.
+    tables[i] is the table of key i.  Returns the fields of the JSON line."""
     import torch
 
-    from morphogen_b200 import gpu_dpf as G
-
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(local_rank)
-
-    wl = WORKLOADS[args.workload]
-    nq = args.queries if args.workload == "batched31" else 1
-    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
-    scanner = G.GpuScanner(local_rank)
-    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
-    k0, k1, targets = seeded_keys(d, rows, nq)
     nkeys = len(k0)
-
-    # Correctness gate (outside timing): both servers' shares XOR to the targets.
     ws = scanner.workspace()
     ws.set_kernel(args.kernel)
-    ws.set_keys([table] * nkeys, k1)
+    # Correctness gate (outside timing): both servers' shares XOR to the targets.
+    ws.set_keys(tables, k1)
     ws.launch()
     s1 = ws.read()
-    ws.set_keys([table] * nkeys, k0)
+    ws.set_keys(tables, k0)
     ws.launch()
     s0 = ws.read()
-    verified = all(bytes(a ^ b for a, b in zip(x, y)) == table.read_rows(t, 1).tobytes()
-                   for x, y, t in zip(s0, s1, targets))
+    verified = all(bytes(a ^ b for a, b in zip(x, y)) == row for x, y, row in zip(s0, s1, targets_rows))
     if not verified:
         raise SystemExit("bench: shares do not reconstruct the target rows")
     tuned = None
@@ -306,7 +292,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     for _ in range(args.warmup):
-        ws.launch(stream=sh)
+        ws.launch(stream=sh, graph=args.graph)
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -321,9 +307,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     t_start.record(stream)
     for i in range(args.steps):
         ev[i][0].record(stream)
-        ws.launch(stream=sh)
+        ws.launch(stream=sh, graph=args.graph)
         ev[i][1].record(stream)
-        scan_ns.append(ws.last_scan_ns())  # waits for this pass; device time of the scan kernel
+        scan_ns.append(ws.last_scan_ns())  # waits for this pass; device time of the scan kernel(s)
     t_end.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -336,86 +322,148 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         total_ms = float(tt.item())
     ms_per_step = total_ms / args.steps
-    bytes_pass = rows * rb
-    value = world * bytes_pass / (ms_per_step * 1e-3) / 1e9
 
-    # e2e: host keys in, host shares out, through mg_scan.
+    # e2e: host keys in, host shares out, through the one-call entry point.
     e2e_ms = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        shares, _ = scanner.scan_keys(table, k0)
+        shares = scanner.scan_multi(list(zip(tables, k0)))
         dt = (time.perf_counter() - t0) * 1e3
         if i >= args.warmup:
             e2e_ms.append(dt)
-    assert shares == s0
+    if shares != s0:
+        raise SystemExit("bench: e2e shares differ")
     e2e_per = sum(e2e_ms) / len(e2e_ms)
     if dist:
         tt = torch.tensor([e2e_per], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_per = float(tt.item())
-    e2e_value = world * bytes_pass / (e2e_per * 1e-3) / 1e9
+    ws.close()
+    return dict(plan=plan, verified=verified, ms_per_step=ms_per_step, step_ms=step_ms, e2e_ms=e2e_ms,
+                e2e_per=e2e_per, scan_avg_s=sum(scan_ns) / len(scan_ns) * 1e-9, clocks=clk)
 
-    # Rooflines of the dominant kernel.  DRAM traffic per launch: the ratio
-    # measured by ncu on a smaller capture of the same kernel, scaled to the
-    # table bytes of this launch.
+
+def run_gpu(args, rank: int, world: int, local_rank: int):
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local_rank)
+
+    wl = WORKLOADS[args.workload]
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    scanner = G.GpuScanner(local_rank)
+    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
+    qlist = [int(q) for q in str(args.queries).split(",")] if args.workload == "batched31" else [1]
     peaks = measured_peaks()
-    traffic = None
-    try:
-        tr = json.loads((ROOT / "profiles" / "traffic.json").read_text())
-        kname = "scan_warp_kernel" if plan.get("kernel") == 2 else "scan_kernel"
-        rec = tr.get(kname, {})
-        if rec.get("table_bytes"):
-            traffic = round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_pass)
-    except (OSError, ValueError):
-        traffic = None
-    scan_avg_s = sum(scan_ns) / len(scan_ns) * 1e-9
-    achieved_hbm = bytes_pass / scan_avg_s / 1e9
     hbm_peak = float(peaks["hbm_gbs"])
-    nodes = nkeys * ((1 << d) - 1)
     prg_peak = scanner.prg_peak()
-    achieved_nodes = nodes / scan_avg_s
-
+    try:
+        traffic_rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+    except (OSError, ValueError):
+        traffic_rec = {}
+    bytes_pass = rows * rb
+    cpu = None
+    for nq in qlist:
+        k0, k1, targets = seeded_keys(d, rows, nq)
+        nkeys = len(k0)
+        m = measure(args, scanner, [table] * nkeys, k0, k1,
+                    [table.read_rows(t, 1).tobytes() for t in targets], world, local_rank, dist)
+        plan = m["plan"]
+        value = world * bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9
+        e2e_value = world * bytes_pass / (m["e2e_per"] * 1e-3) / 1e9
+        # Rooflines of the dominant kernel; DRAM traffic per launch is the
+        # ratio ncu measured on a smaller capture of the same kernel, scaled.
+        achieved_hbm = bytes_pass / m["scan_avg_s"] / 1e9
+        rec = traffic_rec.get("scan_warp_kernel" if plan.get("kernel") == 2 else "scan_kernel", {})
+        traffic = (round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_pass)
+                   if rec.get("table_bytes") and nkeys == 3 else None)
+        nodes = nkeys * ((1 << d) - 1)
+        achieved_nodes = nodes / m["scan_avg_s"]
+        if rank != 0:
+            continue
+        if cpu is None and world == 1 and not args.no_cpu:
+            rates, threads, desc = cpu_scan_sample(k0[:3], rows, rb, min(CPU_SAMPLE_ROWS, rows))
+            cpu = {"value": round(rates[0], 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc}
+        pct = lambda xs, q: float(np.percentile(np.array(xs), q))  # noqa: E731
+        line = {
+            "metric": "scanned GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(m["ms_per_step"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nkeys,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "cuda_graph": bool(args.graph), "plan": plan,
+                       "l2": "inputs larger than L2" if bytes_pass > 126e6 else "table fits L2"},
+            "latency_ms": {"p50": round(pct(m["step_ms"], 50), 3), "p99": round(pct(m["step_ms"], 99), 3),
+                           "e2e_p50": round(pct(m["e2e_ms"], 50), 3), "e2e_p99": round(pct(m["e2e_ms"], 99), 3)},
+            "queries_per_s": round(world * nq / (m["ms_per_step"] * 1e-3), 3),
+            "per_key_GBps": round(value * nkeys, 2),
+            "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
+                    "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
+            "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
+                         "frac": round(achieved_hbm / hbm_peak, 4), "traffic": traffic,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
+                         if "fallback" not in peaks else "fallback 6650 GB/s"},
+            "alu": {"bound": "int32 ALU pipe (ChaCha8)", "achieved": round(achieved_nodes / 1e9, 3),
+                    "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
+                    "frac": round(achieved_nodes / prg_peak, 4),
+                    "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run"},
+            "gpu_launches": plan["kernels"] * args.steps,
+            "clocks": m["clocks"],
+            "verified": m["verified"],
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    if rank != 0:
-        return
 
-    cpu = None
-    if world == 1 and not args.no_cpu:
-        rates, threads, desc = cpu_scan_sample(k0, rows, rb, min(CPU_SAMPLE_ROWS, rows))
-        cpu = {"value": round(rates[0], 4), "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": desc}
 
+def run_mixed(args, local_rank: int):
+    """Two resident tables in one pass: accounts 2^28 x 64 B (28-bit keys) and
+    storage 2^31 x 32 B (31-bit keys); queries per table drawn from U{1..32}."""
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+
+    torch.cuda.set_device(local_rank)
+    scanner = G.GpuScanner(local_rank)
+    acc = G.GpuPageMatrix.from_seed(scanner, 1 << 28, 64, seed=SEED)
+    sto = G.GpuPageMatrix.from_seed(scanner, 1 << 31, 32, seed=SEED + 1)
+    rng = np.random.default_rng(SEED)
+    qa, qs = int(rng.integers(1, 33)), int(rng.integers(1, 33))
+    a0, a1, at = seeded_keys(28, 1 << 28, qa, seed=SEED + 2)
+    s0_, s1_, st_ = seeded_keys(31, 1 << 31, qs, seed=SEED + 3)
+    tables = [acc] * len(a0) + [sto] * len(s0_)
+    rows = [acc.read_rows(t, 1).tobytes() for t in at] + [sto.read_rows(t, 1).tobytes() for t in st_]
+    m = measure(args, scanner, tables, a0 + s0_, a1 + s1_, rows, 1, local_rank, None)
+    bytes_pass = (1 << 28) * 64 + (1 << 31) * 32
+    nodes = len(a0) * ((1 << 28) - 1) + len(s0_) * ((1 << 31) - 1)
+    prg_peak = scanner.prg_peak()
     pct = lambda xs, q: float(np.percentile(np.array(xs), q))  # noqa: E731
     line = {
-        "metric": "scanned GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic",
-        "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nkeys,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "plan": plan, "l2": "inputs larger than L2 (64 GiB table)" if bytes_pass > 126e6
-                   else "table fits L2"},
-        "latency_ms": {"p50": round(pct(step_ms, 50), 3), "p99": round(pct(step_ms, 99), 3),
-                       "e2e_p50": round(pct(e2e_ms, 50), 3), "e2e_p99": round(pct(e2e_ms, 99), 3)},
-        "queries_per_s": round(world * nq / (ms_per_step * 1e-3), 3),
-        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
-                "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
-        "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved_hbm / hbm_peak, 4), "traffic": traffic,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
-                     if "fallback" not in peaks else "fallback 6650 GB/s"},
-        "alu": {"bound": "int32 issue (ChaCha8)", "achieved": round(achieved_nodes / 1e9, 3),
-                "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
-                "frac": round(achieved_nodes / prg_peak, 4),
-                "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run"},
-        "gpu_launches": plan["kernels"] * args.steps,
-        "clocks": clk,
-        "verified": verified,
+        "metric": "queries/s, mixed tables in one pass", "value": round((qa + qs) / (m["ms_per_step"] * 1e-3), 3),
+        "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(m["ms_per_step"], 3), "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "accounts 2^28 x 64 B (28-bit keys) + storage 2^31 x 32 B (31-bit keys), "
+                               "queries per table per pass from U{1..32}",
+                   "accounts_queries": qa, "storage_queries": qs, "keys": 3 * (qa + qs), "plan": m["plan"]},
+        "scanned_GBps": round(bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9, 2),
+        "latency_ms": {"p50": round(pct(m["step_ms"], 50), 3), "e2e_p50": round(pct(m["e2e_ms"], 50), 3)},
+        "alu": {"achieved": round(nodes / m["scan_avg_s"] / 1e9, 3), "peak": round(prg_peak / 1e9, 3),
+                "unit": "G node expansions/s", "frac": round(nodes / m["scan_avg_s"] / prg_peak, 4)},
+        "verified": m["verified"], "clocks": m["clocks"],
     }
-    if cpu:
-        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
 
 
@@ -426,7 +474,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mg", choices=["mg", "reference"])
     ap.add_argument("--workload", default="plain31", choices=sorted(WORKLOADS))
-    ap.add_argument("--queries", type=int, default=1)
+    ap.add_argument("--queries", default="1", help="batched31: queries per pass, or a comma list to sweep")
+    ap.add_argument("--graph", action="store_true", help="replay the timed passes from a CUDA graph")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--autotune", type=int, default=-1,
                     help="autotuner budget in ms before timing (-1: 5000 when a pass is under 20 ms, else off)")
@@ -448,6 +497,9 @@ def main():
     elif args.workload == "serve31":
         if rank == 0:
             run_serve(args, local_rank)
+    elif args.workload == "mixed":
+        if rank == 0:
+            run_mixed(args, local_rank)
     else:
         run_gpu(args, rank, world, local_rank)
 
