@@ -92,12 +92,20 @@ int mg_device_info(mg_context* ctx, int* sm_count, uint64_t* free_bytes, uint64_
 /* ---- tables: GpuPageMatrix (crates/morphogen-gpu-dpf/src/storage.rs) ------ */
 /* alloc_empty (storage.rs:89-101): zero-filled rows x row_bytes on the device. */
 int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table** out);
+/* A table holding rows [first_row, first_row + rows) of a larger logical
+ * table: keys are evaluated at the logical row indices, so the shares of the
+ * range tables that partition a table XOR to the share of the whole table
+ * (sharding one table over several GPUs: per-GPU shares, then one XOR). */
+int mg_table_create_range(mg_context* ctx, uint64_t first_row, uint64_t rows, uint32_t row_bytes,
+                          mg_table** out);
+uint64_t mg_table_first_row(const mg_table* table);
 int mg_table_destroy(mg_table* table);
 /* update_pages (storage.rs:104-124) / new (storage.rs:27-43): host -> device. */
 int mg_table_write_rows(mg_table* table, uint64_t first_row, const void* host_rows, uint64_t nrows);
 int mg_table_read_rows(const mg_table* table, uint64_t first_row, void* host_rows, uint64_t nrows);
-/* Synthetic content: byte o = byte (o % 8) of SplitMix64 output o / 8 of the
- * stream seeded with `seed`; generated on the device. */
+/* Synthetic content: logical byte o (row-range tables start at first_row *
+ * row_bytes) = byte (o % 8) of SplitMix64 output o / 8 of the stream seeded
+ * with `seed`; generated on the device. */
 int mg_table_fill_splitmix(mg_table* table, uint64_t seed);
 /* Epoch merge: row_idx[i] ^= diffs[i] for n entries, in place on the device
  * (the GPU half of EpochManager::try_advance, server/epoch.rs:516-545, and

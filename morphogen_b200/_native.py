@@ -28,7 +28,7 @@ MAX_ROW_BYTES = 4096
 # Every symbol include/morphogen_gpu.h declares.
 EXPORTED = (
     "mg_context_create", "mg_context_destroy", "mg_last_error", "mg_device_info",
-    "mg_table_create", "mg_table_destroy", "mg_table_write_rows", "mg_table_read_rows",
+    "mg_table_create", "mg_table_create_range", "mg_table_first_row", "mg_table_destroy", "mg_table_write_rows", "mg_table_read_rows",
     "mg_table_fill_splitmix", "mg_table_xor_rows", "mg_table_rows", "mg_table_row_bytes",
     "mg_table_device_ptr", "mg_table_delta_reserve", "mg_table_delta_push", "mg_table_delta_count",
     "mg_table_delta_clear", "mg_table_delta_merge", "mg_table_epoch", "mg_key_size", "mg_key_check", "mg_keygen", "mg_scan",
@@ -113,6 +113,8 @@ def lib():
             "mg_last_error": ([], C.c_char_p),
             "mg_device_info": ([vp, C.POINTER(C.c_int), u64p, u64p], C.c_int),
             "mg_table_create": ([vp, C.c_uint64, C.c_uint32, C.POINTER(vp)], C.c_int),
+            "mg_table_create_range": ([vp, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(vp)], C.c_int),
+            "mg_table_first_row": ([vp], C.c_uint64),
             "mg_table_destroy": ([vp], C.c_int),
             "mg_table_write_rows": ([vp, C.c_uint64, vp, C.c_uint64], C.c_int),
             "mg_table_read_rows": ([vp, C.c_uint64, vp, C.c_uint64], C.c_int),

@@ -150,6 +150,7 @@ struct mg_table {
   int device = 0;
   int sms = 0;
   void* d = nullptr;
+  uint64_t first = 0;  // logical index of row 0 (row-range tables)
   uint64_t rows = 0;
   uint32_t row_bytes = 0;
   // Pending epoch delta (DeltaBuffer, crates/morphogen-core/src/delta.rs):
@@ -345,6 +346,15 @@ void shape_for(uint32_t d, uint32_t S_target, uint32_t& S, uint32_t& U, uint32_t
 
 uint64_t ceil_shift(uint64_t x, uint32_t s) { return s >= 64 ? (x ? 1 : 0) : (x + (1ull << s) - 1) >> s; }
 
+// Tree nodes 2^s leaves wide that meet the table's rows [first, first + rows):
+// their first level index and their count.
+uint64_t level_first(const mg_table* t, uint32_t s) { return s >= 64 ? 0 : t->first >> s; }
+uint64_t level_count(const mg_table* t, uint32_t s) {
+  if (t->rows == 0) return 0;
+  if (s >= 64) return 1;
+  return ((t->first + t->rows - 1) >> s) - (t->first >> s) + 1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -396,19 +406,24 @@ int mg_device_info(mg_context* ctx, int* sm_count, uint64_t* free_bytes, uint64_
 // ---- tables -----------------------------------------------------------------
 
 int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table** out) {
+  return mg_table_create_range(ctx, 0, rows, row_bytes, out);
+}
+
+int mg_table_create_range(mg_context* ctx, uint64_t first_row, uint64_t rows, uint32_t row_bytes, mg_table** out) {
   if (!ctx || !out) return fail(MG_EINVAL, "null argument");
   *out = nullptr;
   if (row_bytes == 0 || row_bytes % 16 != 0 || row_bytes > MG_MAX_ROW_BYTES)
     return fail(MG_EINVAL, "row_bytes %u must be a multiple of 16 in [16, %d]", row_bytes,
                 MG_MAX_ROW_BYTES);
-  if (rows > (1ull << MG_MAX_DOMAIN_BITS))
-    return fail(MG_ERANGE, "%llu rows exceed the 2^%d-row domain limit", (unsigned long long)rows,
-                MG_MAX_DOMAIN_BITS);
+  if (first_row > (1ull << MG_MAX_DOMAIN_BITS) || rows > (1ull << MG_MAX_DOMAIN_BITS) - first_row)
+    return fail(MG_ERANGE, "rows [%llu, %llu) exceed the 2^%d-row domain limit", (unsigned long long)first_row,
+                (unsigned long long)(first_row + rows), MG_MAX_DOMAIN_BITS);
   if (int rc = set_device(ctx)) return rc;
   mg_table* t = new mg_table();
   t->ctx = ctx;
   t->device = ctx->device;
   t->sms = ctx->sms;
+  t->first = first_row;
   t->rows = rows;
   t->row_bytes = row_bytes;
   const size_t bytes = (size_t)rows * row_bytes;
@@ -464,7 +479,9 @@ int mg_table_read_rows(const mg_table* t, uint64_t first, void* host, uint64_t n
 int mg_table_fill_splitmix(mg_table* t, uint64_t seed) {
   if (!t) return fail(MG_EINVAL, "null table");
   if (int rc = set_device(t)) return rc;
-  MG_CUDA(mg::launch_fill_splitmix(t->d, t->rows * t->row_bytes / 8, seed, t->sms, nullptr));
+  // Logical byte offset: a row-range table holds the logical table's rows.
+  MG_CUDA(mg::launch_fill_splitmix(t->d, t->rows * t->row_bytes / 8, seed, t->first * t->row_bytes / 8, t->sms,
+                                   nullptr));
   MG_CUDA(cudaDeviceSynchronize());
   return MG_OK;
 }
@@ -497,6 +514,7 @@ int mg_table_xor_rows(mg_table* t, const uint64_t* idx, const void* diffs, uint6
 }
 
 uint64_t mg_table_rows(const mg_table* t) { return t ? t->rows : 0; }
+uint64_t mg_table_first_row(const mg_table* t) { return t ? t->first : 0; }
 uint32_t mg_table_row_bytes(const mg_table* t) { return t ? t->row_bytes : 0; }
 const void* mg_table_device_ptr(const mg_table* t) { return t ? t->d : nullptr; }
 
@@ -747,6 +765,7 @@ int plan_cta(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t col0
       uint32_t S, U, M;
       shape_for(sp.d, S_target, S, U, M);
       sg.table = reinterpret_cast<const uint4*>(sp.table->d);
+      sg.first = sp.table->first;
       sg.rows = sp.table->rows;
       sg.V = sp.table->row_bytes / 16;
       sg.d = sp.d;
@@ -755,7 +774,7 @@ int plan_cta(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t col0
       sg.M = M;
       sg.g = sp.g;
       sg.groups = (uint32_t)(sp.keys.size() / sp.g);
-      sg.tiles = (uint32_t)ceil_shift(sp.table->rows, S);
+      sg.tiles = (uint32_t)level_count(sp.table, S);
       sg.item_begin = items;
       sg.key_base = (uint32_t)cursor;
       sg.col_base = cols;
@@ -810,7 +829,7 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
     uint32_t slots = 1;
     for (const SegPlan& sp : segs) {
       const uint32_t M = std::min(Mt, sp.d);
-      const uint64_t nF = ceil_shift(sp.table->rows, M);
+      const uint64_t nF = level_count(sp.table, M);
       items += (sp.keys.size() / sp.g) * ((nF + 31) / 32);
       slots = std::max(slots, M);
     }
@@ -825,7 +844,7 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
     uint64_t worst = 0;
     for (const SegPlan& sp : segs) {
       const uint32_t M = std::min(Mt, sp.d);
-      const uint64_t tiles = (ceil_shift(sp.table->rows, M) + 31) / 32;
+      const uint64_t tiles = (level_count(sp.table, M) + 31) / 32;
       const uint64_t groups = sp.keys.size() / sp.g;
       worst += (nw >= groups) ? (tiles + (nw / groups) - 1) / (nw / groups) : (groups * tiles + nw - 1) / nw;
     }
@@ -855,9 +874,10 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
     const SegPlan& sp = segs[si];
     mg::WarpSeg& sg = L.w.seg[si];
     const uint32_t M = std::min(best->M, sp.d);
-    const uint64_t nF = ceil_shift(sp.table->rows, M);
+    const uint64_t nF = level_count(sp.table, M);
     const uint32_t nk = (uint32_t)sp.keys.size();
     sg.table = reinterpret_cast<const uint4*>(sp.table->d);
+    sg.first = sp.table->first;
     sg.rows = sp.table->rows;
     sg.item_begin = items;
     sg.fr_base = fr_cursor;
@@ -884,8 +904,10 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
       const uint32_t c = F ? (st == 0 ? F - 8 * (nsteps - 1) : 8u) : 0u;
       f.L_in = Lv;
       f.c = c;
-      f.n_in = Lv ? ceil_shift(sp.table->rows, sp.d - Lv) : 1;
-      f.n_out = ceil_shift(sp.table->rows, sp.d - (Lv + c));
+      f.n_in = Lv ? level_count(sp.table, sp.d - Lv) : 1;
+      f.in_first = Lv ? level_first(sp.table, sp.d - Lv) : 0;
+      f.n_out = level_count(sp.table, sp.d - (Lv + c));
+      f.out_first = level_first(sp.table, sp.d - (Lv + c));
       const bool last = st + 1 == nsteps;
       f.out_base = last ? fr_cursor : 0;
       f.out_stride = last ? nF : f.n_out;
@@ -937,7 +959,8 @@ static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
   }
   for (const mg_batch::DeltaLaunch& dl : b->deltas)
     MG_CUDA(mg::launch_delta(b->d_keys, b->d_jobs + dl.job0, dl.njobs, dl.table->d_delta_idx, dl.table->d_delta_diff,
-                             dl.table->d_delta_count, dl.table->delta_cap, dl.table->row_bytes / 16, b->d_out, st));
+                             dl.table->d_delta_count, dl.table->delta_cap, dl.table->row_bytes / 16, dl.table->first,
+                             b->d_out, st));
   return MG_OK;
 }
 
@@ -1162,9 +1185,9 @@ int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t*
     if (t->ctx != ctx) return fail(MG_EINVAL, "table of key %u belongs to another context", i);
     if (int rc = parse_key(keys[i], key_lens[i], &parsed[i])) return rc;
     const uint32_t d = parsed[i].domain_bits;
-    if (t->rows > domain_size(d))
-      return fail(MG_ERANGE, "more rows than domain size: %llu rows, key %u has %u domain bits",
-                  (unsigned long long)t->rows, i, d);
+    if (t->first + t->rows > domain_size(d))
+      return fail(MG_ERANGE, "more rows than domain size: rows [%llu, %llu), key %u has %u domain bits",
+                  (unsigned long long)t->first, (unsigned long long)(t->first + t->rows), i, d);
     tabs[i] = t;
   }
   b->in_keys = std::move(parsed);

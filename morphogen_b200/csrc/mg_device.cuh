@@ -142,9 +142,10 @@ __device__ __forceinline__ uint4 xor4(uint4 a, const uint4 b) {
 // share row tiles through L2.
 struct Segment {
   const uint4* table;   // rows * V uint4, row-major
-  uint64_t rows;        // rows scanned (<= 2^d)
+  uint64_t first;       // logical index of table row 0 (row-range tables)
+  uint64_t rows;        // rows scanned (first + rows <= 2^d)
   uint64_t item_begin;  // first global item index of the segment
-  uint32_t tiles;       // ceil(rows / 2^S)
+  uint32_t tiles;       // 2^S-leaf tiles intersecting [first, first + rows)
   uint32_t groups;      // key groups
   uint32_t V;           // uint4 per row (row_bytes / 16), 1..256
   uint32_t d;           // domain bits of every key in the segment
@@ -169,7 +170,7 @@ struct ScanParams {
 // ---- warp-independent scan ------------------------------------------------
 //
 // A frontier holds, for every key, the tree nodes at level F = d - M whose
-// subtrees intersect the table (nF = ceil(rows / 2^M) of them).  A warp work
+// subtrees intersect the table's rows [first, first + rows).  A warp work
 // item is 32 consecutive frontier nodes of one key group ("warp tile", 32 x
 // 2^M rows); each lane walks its node's 2^M leaves depth-first.
 
@@ -177,10 +178,11 @@ constexpr int kWarps = kThreads / 32;
 
 struct WarpSeg {
   const uint4* table;   // rows * V uint4
+  uint64_t first;       // logical index of table row 0
   uint64_t rows;
   uint64_t item_begin;  // first global item of the segment
   uint64_t fr_base;     // frontier index of the segment's key 0 (key j at fr_base + j * nF)
-  uint64_t nF;          // frontier nodes per key
+  uint64_t nF;          // frontier nodes per key (level d - M nodes meeting the rows)
   uint32_t tiles;       // warp tiles per key group = ceil(nF / 32)
   uint32_t groups;      // key groups (items are group-major)
   uint32_t d;           // domain bits
@@ -212,6 +214,8 @@ struct FrontierStep {
   const uint8_t* in_t;
   uint4* out_seed;        // key j at out_base + j * out_stride
   uint8_t* out_t;
+  uint64_t in_first;      // level index of input slot 0
+  uint64_t out_first;     // level index of output slot 0
   uint64_t n_in;
   uint64_t n_out;
   uint64_t out_base;

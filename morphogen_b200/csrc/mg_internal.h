@@ -16,7 +16,7 @@ int scan_occupancy(int G, size_t smem);
 cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st);
 cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
                           cudaStream_t st);
-cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, int sms, cudaStream_t st);
+cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, uint64_t word0, int sms, cudaStream_t st);
 cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const void* diffs,
                             uint64_t n, int sms, cudaStream_t st);
 cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
@@ -33,8 +33,8 @@ cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st);
 // Folds a table's pending delta into the shares: jobs[j] = (key slot, first share column).
 cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, const uint64_t* idx,
-                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint4* out,
-                         cudaStream_t st);
+                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint64_t first,
+                         uint4* out, cudaStream_t st);
 
 }  // namespace mg
 

@@ -42,10 +42,11 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
     while (si + 1 < p.nsegs && item >= p.seg[si + 1].item_begin) ++si;
     const Segment& sg = p.seg[si];
     const uint64_t local = item - sg.item_begin;
-    const uint32_t tile = (uint32_t)(local / sg.groups);
     const uint32_t group = (uint32_t)(local % sg.groups);
     const uint32_t g = sg.g, V = sg.V, d = sg.d, S = sg.S, U = sg.U, M = sg.M;
     const uint32_t L0 = d - S;
+    // Global index of the tile at level L0 (row-range tables start mid-domain).
+    const uint32_t tile = (uint32_t)(local / sg.groups + (sg.first >> S));
 
     __syncthreads();  // the previous item is done with shared memory
     {
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
     for (int k = 0; k < G; ++k) acc[k] = make_uint4(0u, 0u, 0u, 0u);
     const uint32_t NR = 1u << U;
     const uint32_t pairs = M ? (1u << (M - 1)) : 1u;
-    const uint64_t tile_row0 = (uint64_t)tile << S;
+    const uint64_t tile_row0 = ((uint64_t)tile << S) - sg.first;  // table row of the tile's first leaf (may wrap)
     const uint32_t rpi = kThreads / V;  // rows per scan sweep
     const uint32_t lane = tid % V, rslot = tid / V;
     const bool scan_thread = tid < rpi * V;
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             const uint32_t r = rb + (uint32_t)u * rpi;
+            // Leaves before the table's first row wrap to huge values and fail the check.
             const uint64_t row = tile_row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
             dat[u] = (r < 2 * NR && row < nrows) ? __ldg(tbl + row * V + lane) : make_uint4(0u, 0u, 0u, 0u);
           }
@@ -213,16 +215,18 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
 
 // ---- warp-independent path -------------------------------------------------
 
-// Frontier chain step: CTA (node, key) expands node `blockIdx.x` of level
-// L_in of key `blockIdx.y` by c <= 8 levels breadth-first in shared memory
-// and stores the nodes of level L_in + c that intersect the table.
+// Frontier chain step: CTA (node, key) expands input slot `blockIdx.x` (level
+// index in_first + slot) of level L_in of key `blockIdx.y` by c <= 8 levels
+// breadth-first in shared memory and stores the nodes of level L_in + c that
+// intersect the table, at slot (level index - out_first).
 __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constant__ FrontierStep f) {
   __shared__ uint4 sa[kThreads], sb[kThreads];
   __shared__ uint8_t ta[kThreads], tb[kThreads];
   const uint32_t tid = threadIdx.x;
   const uint64_t node = blockIdx.x, j = blockIdx.y;
-  const uint64_t out0 = node << f.c;
-  if (out0 >= f.n_out) return;  // uniform per CTA
+  const uint64_t g_out0 = (f.in_first + node) << f.c;  // level index of the first child
+  const uint64_t n = 1ull << f.c;
+  if (g_out0 + n <= f.out_first || g_out0 >= f.out_first + f.n_out) return;  // uniform per CTA
   const KeyDev* __restrict__ K = f.keys + j;
   if (tid == 0) {
     if (f.L_in == 0) {
@@ -250,9 +254,8 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
     uint4* x = cs; cs = ns; ns = x;
     uint8_t* y = ct; ct = nt; nt = y;
   }
-  const uint32_t n = 1u << f.c;
   for (uint32_t i = tid; i < n; i += kThreads) {
-    const uint64_t o = out0 + i;
+    const uint64_t o = g_out0 + i - f.out_first;  // wraps for children before the range
     if (o < f.n_out) {
       f.out_seed[f.out_base + j * f.out_stride + o] = cs[i];
       f.out_t[f.out_base + j * f.out_stride + o] = ct[i];
@@ -369,7 +372,8 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
     }
     const uint4* __restrict__ tbl = sg.table;
     const uint64_t nrows = sg.rows;
-    const uint64_t row0 = (uint64_t)tile << (M + 5);
+    // Table row of the warp tile's first leaf (wraps below the first row).
+    const uint64_t row0 = (((sg.first >> M) + (uint64_t)tile * 32) << M) - sg.first;
     const uint32_t pairs = 1u << (M - 1);
 
     for (uint32_t pi = 0; pi < pairs; ++pi) {
@@ -489,7 +493,7 @@ __device__ __forceinline__ uint4 eval_leaf(const KeyDev* __restrict__ K, uint64_
 // seen by replayed graphs.
 __global__ void __launch_bounds__(kThreads) delta_kernel(const KeyDev* __restrict__ keys, const uint2* __restrict__ jobs,
                                                          const uint64_t* __restrict__ idx, const uint4* __restrict__ diffs,
-                                                         const uint32_t* __restrict__ count, uint32_t V,
+                                                         const uint32_t* __restrict__ count, uint32_t V, uint64_t first,
                                                          uint4* __restrict__ out) {
   __shared__ uint4 s_acc[MG_MAX_ROW_BYTES / 16];
   const uint32_t n = *count;
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) delta_kernel(const KeyDev* __restric
   for (uint32_t v = threadIdx.x; v < V; v += kThreads) s_acc[v] = make_uint4(0u, 0u, 0u, 0u);
   const uint64_t e = e0 + threadIdx.x;
   const bool live = e < n;
-  const uint4 m = live ? eval_leaf(K, idx[e]) : make_uint4(0u, 0u, 0u, 0u);
+  const uint4 m = live ? eval_leaf(K, first + idx[e]) : make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t v = 0; v < V; ++v) {
@@ -541,10 +545,10 @@ __device__ __forceinline__ uint64_t splitmix_word(uint64_t seed, uint64_t w) {
   return z ^ (z >> 31);
 }
 
-__global__ void fill_splitmix_kernel(uint2* __restrict__ dst, uint64_t words, uint64_t seed) {
+__global__ void fill_splitmix_kernel(uint2* __restrict__ dst, uint64_t words, uint64_t seed, uint64_t word0) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
-    const uint64_t z = splitmix_word(seed, w);
+    const uint64_t z = splitmix_word(seed, word0 + w);
     dst[w] = make_uint2((uint32_t)z, (uint32_t)(z >> 32));
   }
 }
@@ -691,12 +695,12 @@ cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, int sms, cudaStream_t st) {
+cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, uint64_t word0, int sms, cudaStream_t st) {
   if (words == 0) return cudaSuccess;
   uint64_t blocks = (words + 255) / 256;
   const uint64_t cap = (uint64_t)sms * 16;
   if (blocks > cap) blocks = cap;
-  fill_splitmix_kernel<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<uint2*>(dst), words, seed);
+  fill_splitmix_kernel<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<uint2*>(dst), words, seed, word0);
   return cudaGetLastError();
 }
 
@@ -779,11 +783,12 @@ cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32
 }
 
 cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, const uint64_t* idx,
-                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint4* out,
-                         cudaStream_t st) {
+                         const void* diffs, const uint32_t* count, uint32_t capacity, uint32_t V, uint64_t first,
+                         uint4* out, cudaStream_t st) {
   if (njobs == 0 || capacity == 0) return cudaSuccess;
   dim3 grid((capacity + kThreads - 1) / kThreads, njobs);
-  delta_kernel<<<grid, kThreads, 0, st>>>(keys, jobs, idx, reinterpret_cast<const uint4*>(diffs), count, V, out);
+  delta_kernel<<<grid, kThreads, 0, st>>>(keys, jobs, idx, reinterpret_cast<const uint4*>(diffs), count, V, first,
+                                          out);
   return cudaGetLastError();
 }
 

@@ -270,7 +270,7 @@ int mg_server_submit(mg_server* s, const mg_table* const* tables, const uint8_t*
       delete r;
       return rc;
     }
-    if (d < 64 && mg_table_rows(tables[i]) > (1ull << d)) {
+    if (d < 64 && mg_table_first_row(tables[i]) + mg_table_rows(tables[i]) > (1ull << d)) {
       delete r;
       mg::set_last_error("more rows than domain size");
       return MG_ERANGE;

@@ -247,13 +247,20 @@ class _Context:
 class GpuPageMatrix:
     """storage.rs:18-124: a device-resident table of `num_pages` rows of `row_bytes`."""
 
-    def __init__(self, scanner: "GpuScanner", num_rows: int, row_bytes: int = PAGE_SIZE_BYTES):
+    def __init__(self, scanner: "GpuScanner", num_rows: int, row_bytes: int = PAGE_SIZE_BYTES,
+                 first_row: int = 0):
         self._scanner = scanner  # keeps the context alive
         h = C.c_void_p()
-        N.check(N.lib().mg_table_create(scanner._ctx.handle, num_rows, row_bytes, C.byref(h)))
+        N.check(N.lib().mg_table_create_range(scanner._ctx.handle, first_row, num_rows, row_bytes, C.byref(h)))
         self.handle = h
         self.row_bytes = row_bytes
+        self.first_row = first_row
         self._rows = num_rows
+
+    @classmethod
+    def range(cls, scanner: "GpuScanner", first_row: int, num_rows: int, row_bytes: int) -> "GpuPageMatrix":
+        """Rows [first_row, first_row + num_rows) of a larger logical table (a shard)."""
+        return cls(scanner, num_rows, row_bytes, first_row)
 
     # storage.rs:27-43
     @classmethod
@@ -272,8 +279,10 @@ class GpuPageMatrix:
         return cls(scanner, num_rows, row_bytes)
 
     @classmethod
-    def from_seed(cls, scanner: "GpuScanner", num_rows: int, row_bytes: int, seed: int) -> "GpuPageMatrix":
-        m = cls(scanner, num_rows, row_bytes)
+    def from_seed(cls, scanner: "GpuScanner", num_rows: int, row_bytes: int, seed: int,
+                  first_row: int = 0) -> "GpuPageMatrix":
+        """Synthetic SplitMix64 rows; a row-range table gets the logical table's rows."""
+        m = cls(scanner, num_rows, row_bytes, first_row)
         m.fill_splitmix(seed)
         return m
 
