@@ -14,11 +14,14 @@ measured HBM copy bandwidth, and `alu` reports it against the ChaCha8 PRG
 ceiling measured in the same run (the binding resource on this workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload plain31|plain20|batched31 --queries Q]
+                  [--workload plain31|plain20|batched31 --queries Q|sharded31|mixed|serve31]
 
-Multi-GPU (torchrun, one process per GPU): every rank serves an independent
-replica of the table (replicas only; the path needs no collective), timing is
-the max over ranks and `value` the aggregate over all replicas.
+Multi-GPU (torchrun, one process per GPU): by default every rank serves an
+independent replica of the table (no collective; weak scaling), timing is the
+max over ranks and `value` the aggregate over all replicas.  `sharded31`
+splits the one table into contiguous row ranges over the ranks instead; each
+pass ends with an NCCL all-gather + XOR of the ranks' shares (strong scaling:
+the per-query latency falls with N).
 """
 from __future__ import annotations
 
@@ -46,6 +49,8 @@ WORKLOADS = {
                     rows=1 << 20, row_bytes=256, d=20),
     "batched31": dict(name="batched queries per pass, 2^31 rows x 32 B (64 GiB), 31-bit keys",
                       rows=1 << 31, row_bytes=32, d=31),
+    "sharded31": dict(name="plain single query, 2^31 rows x 32 B (64 GiB) split into contiguous row ranges "
+                           "over the ranks, shares XOR-combined by NCCL all-gather", rows=1 << 31, row_bytes=32, d=31),
     "mixed": dict(name="accounts 2^28 x 64 B + storage 2^31 x 32 B in one pass", rows=0, row_bytes=0, d=0),
     "serve31": dict(name="serving loop over 2^31 rows x 32 B (64 GiB): Poisson arrivals, 1-32 lookups per "
                          "request (geometric, mean 4), 3 x 31-bit keys per lookup, 2^16-row epoch delta "
@@ -255,22 +260,53 @@ def run_serve(args, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
-def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist, cpu_rows=None):
+def expansions(first: int, n: int, d: int) -> int:
+    """Tree nodes expanded by one key over rows [first, first + n): the
+    internal nodes (levels of width 2^1 .. 2^d) whose leaves meet the range."""
+    return sum(((first + n - 1) >> s) - (first >> s) + 1 for s in range(1, d + 1)) if n else 0
+
+
+def target_rows(table, targets, rb: int, dist, local_rank: int) -> list[bytes]:
+    """The logical table's rows at `targets`: read by the rank whose range
+    holds each one, summed over the ranks (zeros elsewhere)."""
+    import torch
+    buf = np.zeros((len(targets), rb), np.int32)
+    for j, t in enumerate(targets):
+        if table.first_row <= t < table.first_row + table.num_pages():
+            buf[j] = table.read_rows(t - table.first_row, 1)
+    if dist:
+        tt = torch.from_numpy(buf).to(f"cuda:{local_rank}")
+        dist.all_reduce(tt)
+        buf = tt.cpu().numpy()
+    return [buf[j].astype(np.uint8).tobytes() for j in range(len(targets))]
+
+
+def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist, combiner=None):
     """One workload point: correctness gate, optional autotune, K timed device
     passes (CUDA events on the launching stream), e2e passes through mg_scan.
-    tables[i] is the table of key i.  Returns the fields of the JSON line."""
+    tables[i] is the table of key i.  With a ShardCombiner every pass is
+    followed by the XOR-combine of the ranks' shares (tables are row ranges of
+    one logical table).  Returns the fields of the JSON line."""
     import torch
 
+    from morphogen_b200.shard import combine_shares
+
     nkeys = len(k0)
+    host_combine = (lambda sh: combine_shares(sh, device=f"cuda:{local_rank}")) if combiner else (lambda sh: sh)
     ws = scanner.workspace()
     ws.set_kernel(args.kernel)
     # Correctness gate (outside timing): both servers' shares XOR to the targets.
     ws.set_keys(tables, k1)
     ws.launch()
-    s1 = ws.read()
+    s1 = host_combine(ws.read())
     ws.set_keys(tables, k0)
     ws.launch()
-    s0 = ws.read()
+    s0_local = ws.read()
+    s0 = host_combine(s0_local)
+    if combiner:
+        combiner.combine(ws)
+        if combiner.out.cpu().numpy().tobytes() != b"".join(s0):
+            raise SystemExit("bench: device combine differs from the host combine")
     verified = all(bytes(a ^ b for a, b in zip(x, y)) == row for x, y, row in zip(s0, s1, targets_rows))
     if not verified:
         raise SystemExit("bench: shares do not reconstruct the target rows")
@@ -283,7 +319,7 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     if budget > 0:
         tuned = ws.autotune(budget)
         ws.launch()
-        if ws.read() != s0:
+        if ws.read() != s0_local:
             raise SystemExit("bench: autotuned shape changed the shares")
     plan = ws.plan()
     if tuned:
@@ -293,6 +329,8 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     sh = stream.cuda_stream
     for _ in range(args.warmup):
         ws.launch(stream=sh, graph=args.graph)
+        if combiner:
+            combiner.combine(ws, stream)
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -308,6 +346,8 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     for i in range(args.steps):
         ev[i][0].record(stream)
         ws.launch(stream=sh, graph=args.graph)
+        if combiner:
+            combiner.combine(ws, stream)
         ev[i][1].record(stream)
         scan_ns.append(ws.last_scan_ns())  # waits for this pass; device time of the scan kernel(s)
     t_end.record(stream)
@@ -327,7 +367,7 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     e2e_ms = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        shares = scanner.scan_multi(list(zip(tables, k0)))
+        shares = host_combine(scanner.scan_multi(list(zip(tables, k0))))
         dt = (time.perf_counter() - t0) * 1e3
         if i >= args.warmup:
             e2e_ms.append(dt)
@@ -347,6 +387,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
 
     from morphogen_b200 import gpu_dpf as G
+    from morphogen_b200.shard import ShardCombiner, shard_range
 
     dist = None
     if world > 1:
@@ -360,8 +401,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     wl = WORKLOADS[args.workload]
     rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    sharded = args.workload == "sharded31"
+    first, n_local = shard_range(rows, world, rank, 1 << 20) if sharded else (0, rows)
     scanner = G.GpuScanner(local_rank)
-    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
+    table = G.GpuPageMatrix.from_seed(scanner, n_local, rb, seed=SEED, first_row=first)
+    combiner = ShardCombiner(local_rank) if sharded else None
     qlist = [int(q) for q in str(args.queries).split(",")] if args.workload == "batched31" else [1]
     peaks = measured_peaks()
     hbm_peak = float(peaks["hbm_gbs"])
@@ -375,18 +419,24 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     for nq in qlist:
         k0, k1, targets = seeded_keys(d, rows, nq)
         nkeys = len(k0)
-        m = measure(args, scanner, [table] * nkeys, k0, k1,
-                    [table.read_rows(t, 1).tobytes() for t in targets], world, local_rank, dist)
+        m = measure(args, scanner, [table] * nkeys, k0, k1, target_rows(table, targets, rb, dist, local_rank),
+                    world, local_rank, dist, combiner)
         plan = m["plan"]
-        value = world * bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9
-        e2e_value = world * bytes_pass / (m["e2e_per"] * 1e-3) / 1e9
-        # Rooflines of the dominant kernel; DRAM traffic per launch is the
-        # ratio ncu measured on a smaller capture of the same kernel, scaled.
-        achieved_hbm = bytes_pass / m["scan_avg_s"] / 1e9
+        # Replicas: every rank scans the whole table for its own queries (the
+        # aggregate counts each rank's pass).  Sharded: the ranks together
+        # scan the table once per pass.
+        copies = 1 if sharded else world
+        value = copies * bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9
+        e2e_value = copies * bytes_pass / (m["e2e_per"] * 1e-3) / 1e9
+        # Rooflines of the dominant kernel (this rank's launch); DRAM traffic
+        # per launch is the ratio ncu measured on a smaller capture of the
+        # same kernel, scaled.
+        local_bytes = n_local * rb
+        achieved_hbm = local_bytes / m["scan_avg_s"] / 1e9
         rec = traffic_rec.get("scan_warp_kernel" if plan.get("kernel") == 2 else "scan_kernel", {})
-        traffic = (round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_pass)
+        traffic = (round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * local_bytes)
                    if rec.get("table_bytes") and nkeys == 3 else None)
-        nodes = nkeys * ((1 << d) - 1)
+        nodes = nkeys * expansions(first, n_local, d)
         achieved_nodes = nodes / m["scan_avg_s"]
         if rank != 0:
             continue
@@ -397,15 +447,17 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         line = {
             "metric": "scanned GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(m["ms_per_step"], 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
             "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nkeys,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "parallelism": (f"row ranges x{world}" if sharded else f"replicas x{world}")
+                       if world > 1 else "single GPU",
+                       "rows_per_rank": n_local,
                        "cuda_graph": bool(args.graph), "plan": plan,
                        "l2": "inputs larger than L2" if bytes_pass > 126e6 else "table fits L2"},
             "latency_ms": {"p50": round(pct(m["step_ms"], 50), 3), "p99": round(pct(m["step_ms"], 99), 3),
                            "e2e_p50": round(pct(m["e2e_ms"], 50), 3), "e2e_p99": round(pct(m["e2e_ms"], 99), 3)},
-            "queries_per_s": round(world * nq / (m["ms_per_step"] * 1e-3), 3),
+            "queries_per_s": round(copies * nq / (m["ms_per_step"] * 1e-3), 3),
             "per_key_GBps": round(value * nkeys, 2),
             "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
@@ -427,6 +479,39 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_emulated_shards(args, local_rank: int):
+    """sharded31 on one GPU, rank by rank: the row range of every rank of an
+    R-rank job is created, timed and freed in turn (no collective).  Prints
+    one line per R with the slowest range's pass time -- the per-rank compute
+    of the R-GPU job; the all-gather of 3 x 32 B is not included."""
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+    from morphogen_b200.shard import shard_range
+
+    torch.cuda.set_device(local_rank)
+    wl = WORKLOADS["sharded31"]
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    scanner = G.GpuScanner(local_rank)
+    k0, k1, targets = seeded_keys(d, rows, 1)
+    for R in [int(x) for x in str(args.emulate_ranks).split(",")]:
+        per_rank = []
+        for r in range(R):
+            first, n = shard_range(rows, R, r, 1 << 20)
+            t = G.GpuPageMatrix.from_seed(scanner, n, rb, seed=SEED, first_row=first)
+            m = measure(args, scanner, [t] * len(k0), k0, k1, target_rows(t, targets, rb, None, local_rank),
+                        1, local_rank, None)
+            per_rank.append({"first_row": first, "rows": n, "ms_per_step": round(m["ms_per_step"], 3),
+                             "e2e_ms": round(m["e2e_per"], 3), "clocks_sm_mhz": m["clocks"]["sm_mhz"]})
+            t.close()
+        worst = max(x["ms_per_step"] for x in per_rank)
+        print(json.dumps({
+            "metric": "scanned GB/s (per-rank compute of an R-GPU row-range job, ranks emulated one after another "
+                      "on one GPU)", "emulated_ranks": R, "value": round(rows * rb / (worst * 1e-3) / 1e9, 2),
+            "unit": "GB/s", "ms_per_step_slowest_rank": worst, "ranks": per_rank,
+            "config": {"workload": wl["name"], "keys": len(k0)}}), flush=True)
 
 
 def run_mixed(args, local_rank: int):
@@ -484,6 +569,8 @@ def main():
     ap.add_argument("--duration", type=float, default=20.0, help="serve31: seconds of arrivals per rate")
     ap.add_argument("--overload-duration", type=float, default=1.0,
                     help="serve31: seconds of arrivals for rates above capacity")
+    ap.add_argument("--emulate-ranks", default="",
+                    help="sharded31 on one GPU: time every rank's row range of R-rank jobs (comma list of R)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "cta", "warp"],
                     help="scan kernel for the device-resident passes (default: the planner's choice)")
     args = ap.parse_args()
@@ -497,6 +584,8 @@ def main():
     elif args.workload == "serve31":
         if rank == 0:
             run_serve(args, local_rank)
+    elif args.workload == "sharded31" and args.emulate_ranks and world == 1:
+        run_emulated_shards(args, local_rank)
     elif args.workload == "mixed":
         if rank == 0:
             run_mixed(args, local_rank)

@@ -39,6 +39,8 @@ def combine_shares(local: list[bytes], group=None, device=None) -> list[bytes]:
     import torch
     import torch.distributed as dist
 
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return list(local)
     sizes = [len(s) for s in local]
     flat = np.frombuffer(b"".join(local), np.uint8)
     t = torch.from_numpy(flat.copy())
@@ -55,3 +57,76 @@ def combine_shares(local: list[bytes], group=None, device=None) -> list[bytes]:
         out.append(acc[off:off + n].tobytes())
         off += n
     return out
+
+
+def device_view(ptr: int, nbytes: int, device: int):
+    """A torch uint8 tensor over `nbytes` of device memory at `ptr` (no copy)."""
+    import torch
+
+    class _Buf:
+        pass
+
+    b = _Buf()
+    b.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                  "version": 3, "strides": None, "stream": None}
+    return torch.as_tensor(b, device=f"cuda:{device}")
+
+
+def combine_tensor(local, gathered, out, world: int, group=None):
+    """out = XOR over the ranks of `local` (uint8 tensors; `gathered` holds
+    world x local.numel() bytes).  Device tensors go over NCCL, host tensors
+    over gloo."""
+    import torch
+    import torch.distributed as dist
+
+    if world == 1:
+        out.copy_(local)
+        return out
+    dist.all_gather_into_tensor(gathered, local, group=group)
+    parts = gathered.view(world, -1)
+    torch.bitwise_xor(parts[0], parts[1], out=out)
+    for r in range(2, world):
+        out.bitwise_xor_(parts[r])
+    return out
+
+
+class ShardCombiner:
+    """XOR-combines a workspace's device share buffer across the ranks of a
+    process group, on the device: NCCL all-gather of the shares into one
+    buffer, then an XOR fold over the ranks.  The result stays on the device
+    in `out`; on one rank it is a copy of the local shares."""
+
+    def __init__(self, device: int, group=None):
+        import torch.distributed as dist
+
+        self.device = device
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+        self._key = None
+
+    def _bind(self, ws):
+        import torch
+        ptr, n = ws.shares_device()
+        if self._key != (ptr, n):
+            self.local = device_view(ptr, n, self.device)
+            self.gathered = torch.empty(self.world * n, dtype=torch.uint8, device=f"cuda:{self.device}")
+            self.out = torch.empty(n, dtype=torch.uint8, device=f"cuda:{self.device}")
+            self._key = (ptr, n)
+
+    def combine(self, ws, stream=None):
+        """Enqueue the combine of `ws`'s last pass on `stream` (a torch stream;
+        the workspace's pass must have been launched on the same stream)."""
+        import torch
+
+        self._bind(ws)
+        with torch.cuda.stream(stream) if stream is not None else _null():
+            combine_tensor(self.local, self.gathered, self.out, self.world, self.group)
+        return self.out
+
+
+class _null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False

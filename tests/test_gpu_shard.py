@@ -85,3 +85,18 @@ def test_range_limits(scanner, oracle_mod):
     got, _ = scanner.scan_keys(t, [k_ok])
     assert len(got[0]) == 32
     t.close()
+
+
+def test_device_combiner_single_rank(scanner, oracle_mod):
+    from morphogen_b200.shard import ShardCombiner
+    rb, nrows, d = 64, 50_000, 16
+    t = G.GpuPageMatrix.from_seed(scanner, nrows, rb, 5)
+    keys = [oracle_keypair(oracle_mod, d, 7 * j, seed=3, i=j)[0] for j in range(3)]
+    ws = scanner.workspace()
+    ws.set_keys([t] * 3, keys)
+    ws.launch()
+    comb = ShardCombiner(scanner.device_ord if hasattr(scanner, "device_ord") else 0)
+    out = comb.combine(ws)
+    assert out.cpu().numpy().tobytes() == b"".join(ws.read())
+    ws.close()
+    t.close()

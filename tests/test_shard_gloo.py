@@ -37,9 +37,15 @@ def _rank_main(rank, world, port, q):
     keys = [oracle_keypair(oracle, d, t, seed=12, i=t)[0] for t in (3, 5000, 9999)]
     local = oracle.scan_fused(keys, host, rb, row_base=first)
     full = combine_shares(local)
+    # The tensor form the device combiner uses (here on host tensors).
+    import torch
+    from morphogen_b200.shard import combine_tensor
+    lt = torch.from_numpy(np.frombuffer(b"".join(local), np.uint8).copy())
+    out = torch.empty_like(lt)
+    combine_tensor(lt, torch.empty(world * lt.numel(), dtype=torch.uint8), out, world)
     if rank == 0:
         whole = oracle.scan_fused(keys, oracle.fill_splitmix(0, rows * rb, 9), rb)
-        q.put(full == whole)
+        q.put(full == whole and out.numpy().tobytes() == b"".join(whole))
     dist.barrier()
     dist.destroy_process_group()
 
