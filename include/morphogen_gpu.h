@@ -95,7 +95,10 @@ int mg_table_create(mg_context* ctx, uint64_t rows, uint32_t row_bytes, mg_table
 /* A table holding rows [first_row, first_row + rows) of a larger logical
  * table: keys are evaluated at the logical row indices, so the shares of the
  * range tables that partition a table XOR to the share of the whole table
- * (sharding one table over several GPUs: per-GPU shares, then one XOR). */
+ * (sharding one table over several GPUs: per-GPU shares, then one XOR).  The
+ * reference only times this layout (crates/morphogen-gpu-dpf/src/bin/
+ * bench_sharded.rs:14-110: a page-range per GPU, scanned from page 0, no
+ * combine); here each range answers at its own logical rows. */
 int mg_table_create_range(mg_context* ctx, uint64_t first_row, uint64_t rows, uint32_t row_bytes,
                           mg_table** out);
 uint64_t mg_table_first_row(const mg_table* table);

@@ -5,6 +5,9 @@ on each GPU, mg_table_create_range); every rank answers the same keys over its
 rows, and the rank shares XOR to the share of the whole table.  NCCL has no
 XOR reduction, so the shares (a few hundred bytes) are all-gathered and XORed
 locally.  With a CPU process group (gloo) the same code runs without GPUs.
+The reference's counterpart is a timing sketch only
+(crates/morphogen-gpu-dpf/src/bin/bench_sharded.rs:14-110: one page range per
+GPU thread, max latency over the threads, no combine).
 """
 from __future__ import annotations
 
