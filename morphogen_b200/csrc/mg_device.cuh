@@ -174,7 +174,11 @@ struct ScanParams {
 // item is 32 consecutive frontier nodes of one key group ("warp tile", 32 x
 // 2^M rows); each lane walks its node's 2^M leaves depth-first.
 
-constexpr int kWarps = kThreads / 32;
+#ifndef MG_WARP_THREADS
+#define MG_WARP_THREADS 256
+#endif
+constexpr int kWarpThreads = MG_WARP_THREADS;  // CTA size of the warp-independent kernel
+constexpr int kWarps = kWarpThreads / 32;
 
 struct WarpSeg {
   const uint4* table;   // rows * V uint4

@@ -18,6 +18,8 @@
 // reduce_kernel XORs the per-CTA partial rows into the shares.  XOR is
 // associative and commutative, so the shares are bit-exact whatever the
 // schedule.  The kernels contain no waits on other CTAs or on the host.
+#include <type_traits>
+
 #include "mg_device.cuh"
 #include "mg_internal.h"
 #include "morphogen_gpu.h"
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
 #endif
 
 template <int G, int VT>
-__global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
+__global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t slots = p.slots;
@@ -375,7 +377,15 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
     // Table row of the warp tile's first leaf (wraps below the first row).
     const uint64_t row0 = (((sg.first >> M) + (uint64_t)tile * 32) << M) - sg.first;
     const uint32_t pairs = 1u << (M - 1);
-
+    // A warp tile whose 32 x 2^M rows all lie in the table takes the
+    // unchecked path: per-lane row pointers advance by one leaf pair per step
+    // (load jj of a step is RPL / 2 producing lanes further on; RPL is even
+    // for rows up to 256 B).
+    const bool full = row0 < nrows && nrows - row0 >= ((uint64_t)32 << M);
+    const uint4* const lp = full ? tbl + (row0 + ((uint64_t)(r0 >> 1) << M) + (r0 & 1u)) * VT + pos : tbl;
+    const size_t jstride = ((size_t)(RPL >> 1) << M) * VT;
+    auto run_steps = [&](auto full_tag) {
+    constexpr bool FULL = decltype(full_tag)::value && (RPL % 2 == 0);
     for (uint32_t pi = 0; pi < pairs; ++pi) {
       // Rows of this step: r = 2 * (producing lane) + leaf.
       uint4 dat[PF > 0 ? PF : 1];
@@ -383,7 +393,12 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
       for (int jj = 0; jj < PF; ++jj) {
         const uint32_t r = r0 + (uint32_t)jj * RPL;
         const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
-        dat[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+        if constexpr (FULL) {
+          (void)row;
+          dat[jj] = __ldg(lp + (size_t)pi * (2 * VT) + (size_t)jj * jstride);
+        } else {
+          dat[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+        }
       }
 #pragma unroll 1
       for (uint32_t k = 0; k < g; ++k) {
@@ -427,7 +442,12 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
         for (int jj = 0; jj < CH; ++jj) {
           const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
           const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
-          more[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+          if constexpr (FULL) {
+            (void)row;
+            more[jj] = __ldg(lp + (size_t)pi * (2 * VT) + (size_t)(j0 + jj) * jstride);
+          } else {
+            more[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+          }
         }
 #pragma unroll
         for (int jj = 0; jj < CH; ++jj) {
@@ -439,6 +459,11 @@ __global__ void __launch_bounds__(kThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel
       }
       __syncwarp();
     }
+    };
+    if (full)
+      run_steps(std::true_type{});
+    else
+      run_steps(std::false_type{});
     }
   }
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
@@ -740,13 +765,13 @@ static cudaError_t warp_prepare_t(size_t smem) {
 template <int G, int VT>
 static int warp_occupancy_t(size_t smem) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_warp_kernel<G, VT>, kThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_warp_kernel<G, VT>, kWarpThreads, smem) != cudaSuccess)
     return 0;
   return n;
 }
 template <int G, int VT>
 static cudaError_t warp_launch_t(const WarpScanParams& p, uint32_t grid, size_t smem, cudaStream_t st) {
-  scan_warp_kernel<G, VT><<<grid, kThreads, smem, st>>>(p);
+  scan_warp_kernel<G, VT><<<grid, kWarpThreads, smem, st>>>(p);
   return cudaGetLastError();
 }
 
