@@ -15,7 +15,9 @@
 //   5. after the last step the per-thread accumulators are XOR-reduced with
 //      warp shuffles and shared memory and folded into this CTA's own row of
 //      the partial buffer (no atomics).
-// reduce_kernel XORs the per-CTA partial rows into the shares.  XOR is
+// reduce_kernel XORs the partial rows (per CTA, or per warp for the warp
+// kernel) into the shares: slices of the rows in parallel, combined with
+// 64-bit XOR atomics into the zeroed shares.  XOR is
 // associative and commutative, so the shares are bit-exact whatever the
 // schedule.  The kernels contain no waits on other CTAs or on the host.
 #include <type_traits>
@@ -265,6 +267,13 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
   }
 }
 
+// out ^= v with two 64-bit XOR atomics.
+__device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
+  unsigned long long* o = reinterpret_cast<unsigned long long*>(out);
+  atomicXor(o, ((unsigned long long)v.y << 32) | v.x);
+  atomicXor(o + 1, ((unsigned long long)v.w << 32) | v.z);
+}
+
 // Warp-independent fused expansion + scan.  Every warp keeps the same key
 // group over consecutive items (see the assignment below), so the
 // accumulators stay in registers; they are flushed (warp shuffle XOR) into
@@ -469,25 +478,29 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
 }
 
-// out[c] = XOR over the nparts per-CTA partial rows.  Block = cpb columns x
-// (kThreads / cpb) slices; the slices are combined in shared memory.
+// out[c] ^= XOR over the nparts partial rows (launch_reduce zeroes out first).
+// Block (x, y) = cpb columns x (kThreads / cpb) slices over the partial rows
+// [y * per_block, (y + 1) * per_block); slices combine in shared memory and
+// each block folds its result into out with XOR atomics.
 __global__ void __launch_bounds__(kThreads) reduce_kernel(const uint4* __restrict__ partial,
                                                           uint32_t nparts, uint32_t cols,
-                                                          uint4* __restrict__ out) {
+                                                          uint32_t per_block, uint4* __restrict__ out) {
   __shared__ uint4 red[kThreads];
   const uint32_t cpb = cols < 32u ? cols : 32u;
   const uint32_t slices = kThreads / cpb;
   const uint32_t cl = threadIdx.x % cpb, sl = threadIdx.x / cpb;
   const uint32_t c = blockIdx.x * cpb + cl;
+  const uint32_t j0 = blockIdx.y * per_block;
+  const uint32_t j1 = min(nparts, j0 + per_block);
   uint4 v = make_uint4(0u, 0u, 0u, 0u);
   if (c < cols && sl < slices)
-    for (uint32_t j = sl; j < nparts; j += slices) v = xor4(v, partial[(size_t)j * cols + c]);
+    for (uint32_t j = j0 + sl; j < j1; j += slices) v = xor4(v, partial[(size_t)j * cols + c]);
   red[threadIdx.x] = v;
   __syncthreads();
   if (threadIdx.x < cpb && c < cols) {
     uint4 r = make_uint4(0u, 0u, 0u, 0u);
     for (uint32_t s = 0; s < slices; ++s) r = xor4(r, red[s * cpb + threadIdx.x]);
-    out[c] = r;
+    xor_out(out + c, r);
   }
 }
 
@@ -714,9 +727,13 @@ cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, 
 
 cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
                           cudaStream_t st) {
-  const uint32_t cpb = cols < 32u ? cols : 32u;
   if (cols == 0) return cudaSuccess;
-  reduce_kernel<<<(cols + cpb - 1) / cpb, kThreads, 0, st>>>(partial, nparts, cols, out);
+  if (cudaError_t e = cudaMemsetAsync(out, 0, (size_t)cols * 16, st)) return e;
+  const uint32_t cpb = cols < 32u ? cols : 32u;
+  const uint32_t slices = kThreads / cpb;
+  const uint32_t per_block = slices * 4;  // at most 4 partial rows per thread
+  const dim3 grid((cols + cpb - 1) / cpb, nparts ? (nparts + per_block - 1) / per_block : 1);
+  reduce_kernel<<<grid, kThreads, 0, st>>>(partial, nparts, cols, per_block, out);
   return cudaGetLastError();
 }
 
