@@ -279,11 +279,13 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
 // accumulators stay in registers; they are flushed (warp shuffle XOR) into
 // the warp's own partial row when the group or segment changes.  Per item each lane loads its
 // frontier node and walks its 2^M leaves depth-first (stack in the warp's
-// shared-memory slice); a step yields one leaf pair per lane for every key,
-// exchanged through shared memory with __syncwarp only, and the warp scans
-// the step's 64 rows (32 runs of 2) with 128-bit loads issued before the
-// ChaCha work.  V = VT uint4 per row (VT divides 32, so a lane always holds
-// the same 16-byte position of a row).
+// shared-memory slice); a step yields one leaf pair per lane for every key.
+// For rows of VT * G <= 2 uint4 each lane ANDs its own two rows with its own
+// masks.  Otherwise the masks are exchanged through shared memory with
+// __syncwarp only, and the warp scans the step's 64 rows (32 runs of 2) with
+// coalesced 128-bit loads; VT divides 32, so a lane always holds the same
+// 16-byte position of a row.  Either way the step's loads are issued before
+// the ChaCha work.
 #ifndef MG_WARP_MIN_BLOCKS
 #define MG_WARP_MIN_BLOCKS 2
 #endif
@@ -313,13 +315,51 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
   constexpr uint32_t RPL = 32 / VT;     // rows covered by one warp-wide load
   const uint32_t pos = lane % VT, r0 = lane / VT;
 
+  // Rows of at most 32 B (one key per warp) or 16 B (two): every lane scans
+  // its own subtree's two rows of the step (64 contiguous bytes, whole
+  // sectors) against its own leaf masks, with no shared-memory exchange and
+  // VT accumulators per key.  Wider rows use the exchange below, which keeps
+  // the loads coalesced and the register count flat.
+  constexpr bool OWN = VT * G <= 2;
+  constexpr int AV = OWN ? VT : 1;
   uint4 acc[G];
+  uint4 own[G][AV];
 #pragma unroll
-  for (int k = 0; k < G; ++k) acc[k] = make_uint4(0u, 0u, 0u, 0u);
+  for (int k = 0; k < G; ++k) {
+    acc[k] = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int v = 0; v < AV; ++v) own[k][v] = make_uint4(0u, 0u, 0u, 0u);
+  }
   int cur_seg = -1;
   uint32_t cur_group = 0;
 
+  auto flush_own = [&](const WarpSeg& sg, uint32_t group) {
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+#pragma unroll
+      for (int v = 0; v < AV; ++v) {
+        uint4 x = own[k][v];
+#pragma unroll
+        for (uint32_t off = 16; off >= 1; off >>= 1) {
+          x.x ^= __shfl_xor_sync(0xFFFFFFFFu, x.x, off);
+          x.y ^= __shfl_xor_sync(0xFFFFFFFFu, x.y, off);
+          x.z ^= __shfl_xor_sync(0xFFFFFFFFu, x.z, off);
+          x.w ^= __shfl_xor_sync(0xFFFFFFFFu, x.w, off);
+        }
+        if ((uint32_t)k < sg.g && lane == (uint32_t)v) {
+          const size_t col = sg.col_base + ((size_t)group * sg.g + k) * VT + v;
+          my_partial[col] = xor4(my_partial[col], x);
+        }
+        own[k][v] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+  };
+
   auto flush = [&](const WarpSeg& sg, uint32_t group) {
+    if constexpr (OWN) {
+      flush_own(sg, group);
+      return;
+    }
 #pragma unroll
     for (int k = 0; k < G; ++k) {
       uint4 v = acc[k];
@@ -393,6 +433,53 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
     const bool full = row0 < nrows && nrows - row0 >= ((uint64_t)32 << M);
     const uint4* const lp = full ? tbl + (row0 + ((uint64_t)(r0 >> 1) << M) + (r0 & 1u)) * VT + pos : tbl;
     const size_t jstride = ((size_t)(RPL >> 1) << M) * VT;
+    // Own-rows path: the lane's first row of the tile (its subtree's leaves).
+    const uint4* const own_lp = full ? tbl + (row0 + ((uint64_t)lane << M)) * VT : tbl;
+    auto run_own = [&](auto full_tag) {
+    constexpr bool FULL = decltype(full_tag)::value;
+    for (uint32_t pi = 0; pi < pairs; ++pi) {
+      uint4 dat[2 * AV];
+#pragma unroll
+      for (int j = 0; j < 2 * AV; ++j) {
+        if constexpr (FULL) {
+          dat[j] = __ldg(own_lp + (size_t)pi * (2 * VT) + j);
+        } else {
+          const uint64_t row = row0 + ((uint64_t)lane << M) + 2u * pi + (uint32_t)(j / AV);
+          dat[j] = row < nrows ? __ldg(tbl + row * VT + (j % AV)) : make_uint4(0u, 0u, 0u, 0u);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < G; ++k) {
+        if ((uint32_t)k >= g) break;
+        const KeyDev* __restrict__ K = kp + k;
+        uint4* col_seed = w_seed + (size_t)k * slots * 32 + lane;
+        uint8_t* col_t = w_t + (size_t)k * slots * 32 + lane;
+        uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
+        uint4 s = col_seed[lvl * 32];
+        uint32_t t = col_t[lvl * 32];
+        uint4 ml, mr;
+        for (;; ++lvl) {
+          uint4 Lc, Rc;
+          uint32_t tl, tr;
+          expand_cw_g(s, t, K, F + lvl, Lc, tl, Rc, tr);
+          if (lvl == M - 1) {
+            ml = leaf_mask_g(Lc, tl, K);
+            mr = leaf_mask_g(Rc, tr, K);
+            break;
+          }
+          col_seed[(lvl + 1) * 32] = Rc;
+          col_t[(lvl + 1) * 32] = (uint8_t)tr;
+          s = Lc;
+          t = tl;
+        }
+#pragma unroll
+        for (int v = 0; v < AV; ++v) {
+          own[k][v] = xor_and(own[k][v], dat[v], ml);
+          own[k][v] = xor_and(own[k][v], dat[AV + v], mr);
+        }
+      }
+    }
+    };
     auto run_steps = [&](auto full_tag) {
     constexpr bool FULL = decltype(full_tag)::value && (RPL % 2 == 0);
     for (uint32_t pi = 0; pi < pairs; ++pi) {
@@ -469,10 +556,17 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
       __syncwarp();
     }
     };
-    if (full)
-      run_steps(std::true_type{});
-    else
-      run_steps(std::false_type{});
+    if constexpr (OWN) {
+      if (full)
+        run_own(std::true_type{});
+      else
+        run_own(std::false_type{});
+    } else {
+      if (full)
+        run_steps(std::true_type{});
+      else
+        run_steps(std::false_type{});
+    }
     }
   }
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
