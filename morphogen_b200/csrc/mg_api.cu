@@ -108,6 +108,22 @@ int parse_key(const uint8_t* b, size_t len, KeyDev* k) {
   return MG_OK;
 }
 
+// The warp kernel's per-key constants (KeyAux): t correction bytes as
+// masks and the four possible last-level XOR terms of a leaf mask.
+void make_aux(const KeyDev& k, mg::KeyAux* a) {
+  std::memset(a, 0, sizeof *a);
+  const auto one = [](uint8_t t) { return t == 1 ? 0xFFFFFFFFu : 0u; };
+  const auto big = [](uint8_t t) { return t >= 2 ? 0xFFFFFFFFu : 0u; };
+  for (uint32_t l = 0; l < k.domain_bits; ++l)
+    a->cw_tm[l] = make_uint4(one(k.cw_tl[l]), big(k.cw_tl[l]), one(k.cw_tr[l]), big(k.cw_tr[l]));
+  const uint4 f = k.final_cw;
+  const uint4 c = k.domain_bits ? k.cw_seed[k.domain_bits - 1] : make_uint4(0u, 0u, 0u, 0u);
+  a->leaf_c[0] = make_uint4(0u, 0u, 0u, 0u);
+  a->leaf_c[1] = f;
+  a->leaf_c[2] = c;
+  a->leaf_c[3] = make_uint4(c.x ^ f.x, c.y ^ f.y, c.z ^ f.z, c.w ^ f.w);
+}
+
 int wait_event(cudaEvent_t ev, uint32_t timeout_ms) {
   if (timeout_ms == 0) {
     MG_CUDA(cudaEventSynchronize(ev));
@@ -275,8 +291,9 @@ int grow(mg_batch* b, size_t nkeys, size_t partial_u4, size_t out_u4, size_t fr_
     b->d_keys = nullptr;
     b->h_keys = nullptr;
     b->cap_keys = 0;
-    if (cudaMalloc(&b->d_keys, nkeys * sizeof(KeyDev)) != cudaSuccess ||
-        cudaMallocHost(&b->h_keys, nkeys * sizeof(KeyDev)) != cudaSuccess) {
+    // Keys, then their warp-kernel constants (KeyAux) right after the pass's keys.
+    const size_t bytes = nkeys * (sizeof(KeyDev) + sizeof(mg::KeyAux));
+    if (cudaMalloc(&b->d_keys, bytes) != cudaSuccess || cudaMallocHost(&b->h_keys, bytes) != cudaSuccess) {
       cudaGetLastError();
       return fail(MG_ENOMEM, "cannot allocate key buffers for %zu keys", nkeys);
     }
@@ -1088,7 +1105,12 @@ int plan_pass(mg_batch* b) {
   size_t max_partial = 0;
   for (const mg_batch::Launch& L : launches) max_partial = std::max(max_partial, (size_t)L.nparts * L.cols);
   if (int rc = grow(b, nkeys, max_partial, total_cols, (size_t)fr_cursor, tmp_need)) return rc;
-  for (uint32_t i = 0; i < nkeys; ++i) b->h_keys[key_slot[i]] = parsed[i];
+  mg::KeyAux* const h_aux = reinterpret_cast<mg::KeyAux*>(b->h_keys + nkeys);
+  const mg::KeyAux* const d_aux = reinterpret_cast<const mg::KeyAux*>(b->d_keys + nkeys);
+  for (uint32_t i = 0; i < nkeys; ++i) {
+    b->h_keys[key_slot[i]] = parsed[i];
+    make_aux(parsed[i], &h_aux[key_slot[i]]);
+  }
   for (mg_batch::Launch& L : launches) {
     if (L.kind == MG_KERNEL_CTA) {
       L.p.keys = b->d_keys;
@@ -1096,6 +1118,7 @@ int plan_pass(mg_batch* b) {
       continue;
     }
     L.w.keys = b->d_keys;
+    L.w.aux = d_aux;
     L.w.fr_seed = b->d_fr_seed;
     L.w.fr_t = b->d_fr_t;
     L.w.partial = b->d_partial;
@@ -1116,8 +1139,8 @@ int plan_pass(mg_batch* b) {
       }
     }
   }
-  MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * sizeof(KeyDev), cudaMemcpyHostToDevice,
-                          b->stream));
+  MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * (sizeof(KeyDev) + sizeof(mg::KeyAux)),
+                          cudaMemcpyHostToDevice, b->stream));
   b->launches = std::move(launches);
   b->total_cols = total_cols;
   b->key_col = std::move(key_col);

@@ -42,6 +42,21 @@ struct alignas(16) KeyDev {
 };
 static_assert(sizeof(KeyDev) == 624, "KeyDev layout");
 
+// Per-key constants of the warp-independent kernel, derived on the host from
+// the key.  That kernel carries a node's t as a mask (all ones iff t == 1);
+// for a parent mask m and the PRG's child bit b, the child's mask is
+//   (-b ^ (one & m)) & ~(big & m)
+// where, per level and side, one = all ones iff the t correction byte is 1
+// and big = all ones iff it is 2..255 (the child's t byte is then >= 2 and
+// never corrects).  This equals the byte rule of dpf.rs:122,192,228 exactly.
+// leaf_c[2 * p + c] = (p ? cw_seed[d - 1] : 0) ^ (c ? final_cw : 0): the
+// leaf mask of a last-level child is its PRG seed XOR leaf_c[parent t, child t].
+struct alignas(16) KeyAux {
+  uint4 cw_tm[kMaxLevels];  // x: tl one, y: tl big, z: tr one, w: tr big (0 or ~0)
+  uint4 leaf_c[4];
+};
+static_assert(sizeof(KeyAux) == 576, "KeyAux layout");
+
 __device__ __forceinline__ uint32_t rotl16(uint32_t x) { return __byte_perm(x, 0, 0x1032); }
 __device__ __forceinline__ uint32_t rotl8(uint32_t x) { return __byte_perm(x, 0, 0x2103); }
 __device__ __forceinline__ uint32_t rotl12(uint32_t x) { return __funnelshift_l(x, x, 12); }
@@ -128,6 +143,37 @@ __device__ __forceinline__ uint4 leaf_mask_g(const uint4 s, const uint32_t t, co
   return make_uint4(s.x ^ (f.x & m), s.y ^ (f.y & m), s.z ^ (f.z & m), s.w ^ (f.w & m));
 }
 
+// expand_cw_g with t carried as a mask (KeyAux): m is all ones iff the
+// parent's t == 1; ml / mr are the children's masks.
+__device__ __forceinline__ void expand_cw_m(const uint4 s, const uint32_t m, const KeyDev* __restrict__ k,
+                                            const KeyAux* __restrict__ a, const uint32_t level, uint4& L,
+                                            uint32_t& ml, uint4& R, uint32_t& mr) {
+  const uint4 cw = __ldg(&k->cw_seed[level]);
+  const uint4 tm = __ldg(&a->cw_tm[level]);
+  uint32_t tl, tr;
+  prg_expand(s, L, R, tl, tr);
+  L.x ^= cw.x & m; L.y ^= cw.y & m; L.z ^= cw.z & m; L.w ^= cw.w & m;
+  R.x ^= cw.x & m; R.y ^= cw.y & m; R.z ^= cw.z & m; R.w ^= cw.w & m;
+  ml = ((0u - tl) ^ (tm.x & m)) & ~(tm.y & m);
+  mr = ((0u - tr) ^ (tm.z & m)) & ~(tm.w & m);
+}
+
+// Last level (level d - 1): both children's leaf masks straight from the PRG
+// seeds, with the level's correction word and the final correction word
+// folded into one table lookup per child.
+__device__ __forceinline__ void leaf_pair_m(const uint4 s, const uint32_t m, const KeyAux* __restrict__ a,
+                                            const uint32_t level, uint4& mask_l, uint4& mask_r) {
+  const uint4 tm = __ldg(&a->cw_tm[level]);
+  uint32_t tl, tr;
+  prg_expand(s, mask_l, mask_r, tl, tr);
+  const uint32_t ml = ((0u - tl) ^ (tm.x & m)) & ~(tm.y & m);
+  const uint32_t mr = ((0u - tr) ^ (tm.z & m)) & ~(tm.w & m);
+  const uint4 cl = __ldg(&a->leaf_c[(m & 2u) | (ml & 1u)]);
+  const uint4 cr = __ldg(&a->leaf_c[(m & 2u) | (mr & 1u)]);
+  mask_l.x ^= cl.x; mask_l.y ^= cl.y; mask_l.z ^= cl.z; mask_l.w ^= cl.w;
+  mask_r.x ^= cr.x; mask_r.y ^= cr.y; mask_r.z ^= cr.z; mask_r.w ^= cr.w;
+}
+
 __device__ __forceinline__ uint4 xor_and(uint4 acc, const uint4 d, const uint4 m) {
   acc.x ^= d.x & m.x; acc.y ^= d.y & m.y; acc.z ^= d.z & m.z; acc.w ^= d.w & m.w;
   return acc;
@@ -200,6 +246,7 @@ struct WarpSeg {
 struct WarpScanParams {
   WarpSeg seg[kMaxSegs];
   const KeyDev* keys;
+  const KeyAux* aux;    // one per key, same index as keys
   const uint4* fr_seed;
   const uint8_t* fr_t;
   uint4* partial;       // [gridDim.x * kWarps][cols]

@@ -293,6 +293,29 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
 #define MG_WARP_PREFETCH 8
 #endif
 
+// One depth-first step of a lane's walk: leaf pair `pi` of the lane's
+// subtree (root at tree level F, M levels deep).  The path re-joins the
+// stack (col_seed / col_t, stride 32) at relative level M - ffs(pi) (the
+// root for pi == 0), pushes the right children it passes and returns the
+// two leaf masks.
+__device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const KeyAux* __restrict__ A,
+                                          uint4* col_seed, int8_t* col_t, uint32_t pi, uint32_t M, uint32_t F,
+                                          uint4& ml, uint4& mr) {
+  uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
+  uint4 s = col_seed[lvl * 32];
+  uint32_t m = (uint32_t)(int32_t)col_t[lvl * 32];
+  for (; lvl < M - 1; ++lvl) {
+    uint4 Lc, Rc;
+    uint32_t mlc, mrc;
+    expand_cw_m(s, m, K, A, F + lvl, Lc, mlc, Rc, mrc);
+    col_seed[(lvl + 1) * 32] = Rc;
+    col_t[(lvl + 1) * 32] = (int8_t)mrc;
+    s = Lc;
+    m = mlc;
+  }
+  leaf_pair_m(s, m, A, F + M - 1, ml, mr);
+}
+
 template <int G, int VT>
 __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -301,8 +324,9 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
   uint4* const base4 = reinterpret_cast<uint4*>(smem_raw);
   uint4* const w_mask = base4 + (size_t)warp * G * 64;                                  // [G][64]
   uint4* const w_seed = base4 + (size_t)kWarps * G * 64 + (size_t)warp * G * slots * 32;  // [G][slots][32]
-  uint8_t* const w_t = reinterpret_cast<uint8_t*>(base4 + (size_t)kWarps * G * 64 + (size_t)kWarps * G * slots * 32) +
-                       (size_t)warp * G * slots * 32;
+  // Stack t masks, one byte each (0 or 0xFF; sign-extended on load).
+  int8_t* const w_t = reinterpret_cast<int8_t*>(base4 + (size_t)kWarps * G * 64 + (size_t)kWarps * G * slots * 32) +
+                      (size_t)warp * G * slots * 32;
 
   const uint64_t gw = (uint64_t)blockIdx.x * kWarps + warp;
   const uint64_t nw = (uint64_t)gridDim.x * kWarps;
@@ -416,10 +440,11 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
     const uint64_t node = (uint64_t)tile * 32 + lane;
     const bool valid = node < sg.nF;
     const KeyDev* __restrict__ kp = p.keys + sg.key_base + (size_t)group * g;
+    const KeyAux* __restrict__ ap = p.aux + sg.key_base + (size_t)group * g;
     for (uint32_t k = 0; k < g; ++k) {
       const uint64_t idx = sg.fr_base + ((uint64_t)group * g + k) * sg.nF + node;
       w_seed[(k * slots) * 32 + lane] = valid ? p.fr_seed[idx] : make_uint4(0u, 0u, 0u, 0u);
-      w_t[(k * slots) * 32 + lane] = valid ? p.fr_t[idx] : (uint8_t)0;
+      w_t[(k * slots) * 32 + lane] = (valid && p.fr_t[idx] == 1) ? (int8_t)-1 : (int8_t)0;
     }
     const uint4* __restrict__ tbl = sg.table;
     const uint64_t nrows = sg.rows;
@@ -451,27 +476,9 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
 #pragma unroll
       for (int k = 0; k < G; ++k) {
         if ((uint32_t)k >= g) break;
-        const KeyDev* __restrict__ K = kp + k;
-        uint4* col_seed = w_seed + (size_t)k * slots * 32 + lane;
-        uint8_t* col_t = w_t + (size_t)k * slots * 32 + lane;
-        uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
-        uint4 s = col_seed[lvl * 32];
-        uint32_t t = col_t[lvl * 32];
         uint4 ml, mr;
-        for (;; ++lvl) {
-          uint4 Lc, Rc;
-          uint32_t tl, tr;
-          expand_cw_g(s, t, K, F + lvl, Lc, tl, Rc, tr);
-          if (lvl == M - 1) {
-            ml = leaf_mask_g(Lc, tl, K);
-            mr = leaf_mask_g(Rc, tr, K);
-            break;
-          }
-          col_seed[(lvl + 1) * 32] = Rc;
-          col_t[(lvl + 1) * 32] = (uint8_t)tr;
-          s = Lc;
-          t = tl;
-        }
+        leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
+                  pi, M, F, ml, mr);
 #pragma unroll
         for (int v = 0; v < AV; ++v) {
           own[k][v] = xor_and(own[k][v], dat[v], ml);
@@ -498,26 +505,11 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
       }
 #pragma unroll 1
       for (uint32_t k = 0; k < g; ++k) {
-        const KeyDev* __restrict__ K = kp + k;
-        uint4* col_seed = w_seed + (size_t)k * slots * 32 + lane;
-        uint8_t* col_t = w_t + (size_t)k * slots * 32 + lane;
-        uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
-        uint4 s = col_seed[lvl * 32];
-        uint32_t t = col_t[lvl * 32];
-        for (;; ++lvl) {
-          uint4 Lc, Rc;
-          uint32_t tl, tr;
-          expand_cw_g(s, t, K, F + lvl, Lc, tl, Rc, tr);
-          if (lvl == M - 1) {
-            w_mask[k * 64 + 2 * lane] = leaf_mask_g(Lc, tl, K);
-            w_mask[k * 64 + 2 * lane + 1] = leaf_mask_g(Rc, tr, K);
-            break;
-          }
-          col_seed[(lvl + 1) * 32] = Rc;
-          col_t[(lvl + 1) * 32] = (uint8_t)tr;
-          s = Lc;
-          t = tl;
-        }
+        uint4 ml, mr;
+        leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
+                  pi, M, F, ml, mr);
+        w_mask[k * 64 + 2 * lane] = ml;
+        w_mask[k * 64 + 2 * lane + 1] = mr;
       }
       __syncwarp();
 #pragma unroll
