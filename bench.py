@@ -117,6 +117,17 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        note = None
+        if not self.lines:
+            # Timed region shorter than the sampling interval: one reading
+            # right after it (the clocks have not settled back to idle yet).
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10)
+                self.lines = [ln.strip() for ln in out.stdout.splitlines() if ln.strip()]
+                note = "timed region shorter than the 100 ms sampling interval; one reading right after it"
+            except (OSError, subprocess.TimeoutExpired):
+                pass
         sm, smax, power, reasons = [], None, [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -132,9 +143,12 @@ class ClockSampler:
             for n, v in zip(names, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm),
-                "power_w_max": max(power) if power else None}
+        res = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+               "reasons": sorted(reasons), "samples": len(sm),
+               "power_w_max": max(power) if power else None}
+        if note:
+            res["note"] = note
+        return res
 
 
 def cpu_scan_sample(keys, rows_total: int, row_bytes: int, sample_rows: int, reps: int = 1):
