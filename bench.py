@@ -14,7 +14,7 @@ measured HBM copy bandwidth, and `alu` reports it against the ChaCha8 PRG
 ceiling measured in the same run (the binding resource on this workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload plain31|plain20|batched31 --queries Q|sharded31|mixed|serve31]
+                  [--workload plain31|plain20|batched31 --queries Q|sharded31|pages|mixed|serve31]
 
 Multi-GPU (torchrun, one process per GPU): by default every rank serves an
 independent replica of the table (no collective; weak scaling), timing is the
@@ -51,6 +51,10 @@ WORKLOADS = {
                       rows=1 << 31, row_bytes=32, d=31),
     "sharded31": dict(name="plain single query, 2^31 rows x 32 B (64 GiB) split into contiguous row ranges "
                            "over the ranks, shares XOR-combined by NCCL all-gather", rows=1 << 31, row_bytes=32, d=31),
+    "pages": dict(name="page mode (the reference's layout): 16,817,159 pages x 4096 B (68.9 GB), 25-bit keys",
+                  rows=16_817_159, row_bytes=4096, d=25),
+    "pages_s": dict(name="profiling case: 2^16 pages x 4096 B (256 MiB) scanned with 25-bit keys",
+                    rows=1 << 16, row_bytes=4096, d=25),
     "mixed": dict(name="accounts 2^28 x 64 B + storage 2^31 x 32 B in one pass", rows=0, row_bytes=0, d=0),
     "serve31": dict(name="serving loop over 2^31 rows x 32 B (64 GiB): Poisson arrivals, 1-32 lookups per "
                          "request (geometric, mean 4), 3 x 31-bit keys per lookup, 2^16-row epoch delta "
@@ -58,8 +62,8 @@ WORKLOADS = {
 }
 KEYS_PER_QUERY = 3
 SEED = 0
-CPU_SAMPLE_ROWS = 1 << 28      # aligned window timed on the host cores (cpu_baseline)
-REF_SAMPLE_ROWS = 1 << 25      # per-step sample of the reference arm
+CPU_SAMPLE_BYTES = 8 << 30     # aligned window timed on the host cores (cpu_baseline): 2^28 rows of 32 B
+REF_SAMPLE_BYTES = 1 << 30     # per-step sample of the reference arm: 2^25 rows of 32 B
 
 
 def measured_peaks() -> dict:
@@ -181,7 +185,7 @@ def run_reference(args, rank: int, world: int):
     wl = WORKLOADS[args.workload]
     nq = int(str(args.queries).split(",")[0]) if args.workload == "batched31" else 1
     k0, _, _ = seeded_keys(wl["d"], wl["rows"], nq)
-    sample = min(REF_SAMPLE_ROWS, wl["rows"])
+    sample = min(REF_SAMPLE_BYTES // wl["row_bytes"], wl["rows"])
     _, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.warmup)
     rates, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.steps)
     v = sum(rates) / len(rates)
@@ -455,7 +459,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         if rank != 0:
             continue
         if cpu is None and world == 1 and not args.no_cpu:
-            rates, threads, desc = cpu_scan_sample(k0[:3], rows, rb, min(CPU_SAMPLE_ROWS, rows))
+            rates, threads, desc = cpu_scan_sample(k0[:3], rows, rb, min(CPU_SAMPLE_BYTES // rb, rows))
             cpu = {"value": round(rates[0], 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc}
         pct = lambda xs, q: float(np.percentile(np.array(xs), q))  # noqa: E731
         line = {
