@@ -273,6 +273,41 @@ class GpuPageMatrix:
         m.update_pages(0, data)
         return m
 
+    # storage.rs:45-86
+    @classmethod
+    def from_chunked_matrix(cls, scanner: "GpuScanner", matrix, row_bytes: int = PAGE_SIZE_BYTES) -> "GpuPageMatrix":
+        """Build from a chunked CPU matrix: `matrix` is a sequence of byte
+        chunks, or an object with num_chunks() / chunk(i) like the storage
+        crate's ChunkedMatrix.  The total is padded with zeros to whole rows;
+        each chunk is uploaded at row offset // row_bytes of its byte offset,
+        a chunk that is not a whole number of rows padded with zeros first."""
+        if hasattr(matrix, "num_chunks"):
+            chunks = [matrix.chunk(i) for i in range(matrix.num_chunks())]
+        else:
+            chunks = list(matrix)
+        views = [np.frombuffer(bytes(c), np.uint8) if not isinstance(c, np.ndarray)
+                 else np.ascontiguousarray(c, dtype=np.uint8).reshape(-1) for c in chunks]
+        total = sum(v.size for v in views)
+        m = cls(scanner, (total + row_bytes - 1) // row_bytes, row_bytes)
+        offset = 0
+        for v in views:
+            size = v.size
+            if size % row_bytes:
+                v = np.concatenate([v, np.zeros(row_bytes - size % row_bytes, np.uint8)])
+            if size:
+                m.update_pages(offset // row_bytes, v)
+            offset += size
+        return m
+
+    @property
+    def device(self) -> int:
+        """CUDA device ordinal holding the table."""
+        return self._scanner.device
+
+    def as_slice(self) -> tuple[int, int]:
+        """(device pointer, bytes) of the resident rows."""
+        return self.device_ptr(), self.size_bytes()
+
     # storage.rs:89-101
     @classmethod
     def alloc_empty(cls, scanner: "GpuScanner", num_rows: int, row_bytes: int = PAGE_SIZE_BYTES):

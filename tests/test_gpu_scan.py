@@ -62,6 +62,9 @@ SWEEP = [
     (48, 10, 1000), (64, 13, 8000), (80, 11, 2048), (256, 14, 16384), (32, 16, 65536),
     (32, 18, 200001), (512, 9, 512), (4096, 10, 700), (1024, 12, 4000), (2048, 8, 256),
     (32, 24, 1 << 20),
+    # the largest domain over small tables (frontier chain past level 31), and
+    # 16-B rows with 31-bit keys
+    (32, 32, 70_001), (16, 32, 3), (16, 31, 100_000), (64, 28, 3000),
 ]
 
 
@@ -293,3 +296,22 @@ def test_autotuner_keeps_shares_and_caches_the_shape(scanner, oracle_mod):
     assert got == oracle_mod.scan_fused(other, rows, 64)
     ws.close()
     ws2.close()
+
+
+def test_from_chunked_matrix_pads_like_the_reference(scanner, oracle_mod):
+    # storage.rs:45-86: chunks uploaded at their byte offsets, the total and a
+    # ragged last chunk padded with zeros to whole pages.
+    rb = 4096
+    data = oracle_mod.fill_splitmix(0, 5 * rb + 1000, 17)
+    chunks = [data[:2 * rb], data[2 * rb:5 * rb], data[5 * rb:]]
+    m = G.GpuPageMatrix.from_chunked_matrix(scanner, chunks, rb)
+    assert m.num_pages() == 6 and m.size_bytes() == 6 * rb
+    want = np.concatenate([data, np.zeros(6 * rb - data.size, np.uint8)])
+    assert (m.read_rows(0, 6) == want).all()
+    ptr, n = m.as_slice()
+    assert ptr == m.device_ptr() and n == 6 * rb and m.device == scanner.device
+    k0, k1 = oracle_keypair(oracle_mod, 3, 5, seed=18)
+    a = scanner.scan_keys(m, [k0])[0][0]
+    b = scanner.scan_keys(m, [k1])[0][0]
+    assert bytes(x ^ y for x, y in zip(a, b)) == want[5 * rb:].tobytes()
+    m.close()

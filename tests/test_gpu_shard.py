@@ -20,6 +20,8 @@ pytestmark = pytest.mark.gpu
     (32, 1 << 18, 18, 2, 1 << 16),       # power-of-two halves
     (32, 300_001, 20, 3, 4096),          # ragged end, domain larger than the table
     (64, 100_000, 17, 2, 1),             # split at an odd row
+    (32, 100_003, 17, 3, 1),             # 32-B rows (own-rows path), odd splits
+    (16, 50_001, 31, 2, 1),              # 16-B rows, 31-bit keys
     (4096, 600, 10, 4, 7),               # page rows, odd boundaries
 ])
 def test_ranges_xor_to_whole_table(scanner, oracle_mod, kernel, rb, nrows, d, world, align):
