@@ -237,9 +237,26 @@ struct mg_batch {
   bool launched = false;
   cudaGraphExec_t gexec = nullptr;
   std::vector<uint8_t> graph_sig;
+  // What the current plan was made for: a later set_keys with the same
+  // tables, key depths, shape and delta buffers only restages the keys.
+  std::vector<uint32_t> plan_slot;     // input key i -> key slot
+  std::vector<uint32_t> plan_depth;    // input key i -> domain bits
+  std::vector<const mg_table*> plan_tables;
+  std::vector<std::pair<const void*, uint32_t>> plan_deltas;  // per input key: delta buffer, capacity
+  std::vector<std::array<uint64_t, 4>> plan_shapes;  // per input key: table memory, rows, row bytes, first row
+  int plan_kind = -1;
+  uint32_t plan_S = 0, plan_G = 0;
+  bool plan_reused = false;           // the last set_keys kept the plan
 };
 
 namespace {
+
+// What a plan depends on in a table besides its identity (a destroyed table's
+// address can come back for a different table).
+std::array<uint64_t, 4> table_shape(const mg_table* t) {
+  return {(uint64_t)(uintptr_t)t->d, t->rows, t->row_bytes, t->first};
+}
+
 
 template <class T>
 int set_device(const T* obj) {
@@ -1143,6 +1160,19 @@ int plan_pass(mg_batch* b) {
                           cudaMemcpyHostToDevice, b->stream));
   b->launches = std::move(launches);
   b->total_cols = total_cols;
+  b->plan_slot = key_slot;
+  b->plan_depth.resize(nkeys);
+  b->plan_deltas.resize(nkeys);
+  for (uint32_t i = 0; i < nkeys; ++i) {
+    b->plan_depth[i] = parsed[i].domain_bits;
+    b->plan_deltas[i] = {b->in_tables[i]->d_delta_idx, b->in_tables[i]->delta_cap};
+  }
+  b->plan_tables = b->in_tables;
+  b->plan_shapes.resize(nkeys);
+  for (uint32_t i = 0; i < nkeys; ++i) b->plan_shapes[i] = table_shape(b->in_tables[i]);
+  b->plan_kind = b->eff_kind;
+  b->plan_S = b->eff_S;
+  b->plan_G = b->eff_G;
   b->key_col = std::move(key_col);
   b->key_bytes = std::move(key_bytes);
   b->total_share_bytes = 0;
@@ -1213,6 +1243,39 @@ int mg_batch_set_keys(mg_batch* b, const mg_table* const* tables, const uint8_t*
                   (unsigned long long)t->first, (unsigned long long)(t->first + t->rows), i, d);
     tabs[i] = t;
   }
+  // Same tables, key depths and delta buffers as the planned pass, and the
+  // same effective shape: keep the plan and its buffers, restage the keys.
+  if (b->planned && tabs == b->plan_tables) {
+    bool same = true;
+    for (uint32_t i = 0; i < nkeys && same; ++i)
+      same = parsed[i].domain_bits == b->plan_depth[i] && b->plan_shapes[i] == table_shape(tabs[i]) &&
+             b->plan_deltas[i] == std::make_pair((const void*)tabs[i]->d_delta_idx, tabs[i]->delta_cap);
+    int kind = b->kind_pref;
+    uint32_t S = b->shape_S, G = b->shape_G;
+    if (same && kind == MG_KERNEL_AUTO && S == 0 && G == 0) {
+      // b->signature is this workload's signature (same tables and depths).
+      std::lock_guard<std::mutex> lk(ctx->tune_mu);
+      auto it = ctx->tuned.find(b->signature);
+      if (it != ctx->tuned.end()) {
+        kind = (int)it->second[0];
+        S = it->second[1];
+        G = it->second[2];
+      }
+    }
+    if (same && kind == b->plan_kind && S == b->plan_S && G == b->plan_G) {
+      mg::KeyAux* const h_aux = reinterpret_cast<mg::KeyAux*>(b->h_keys + nkeys);
+      for (uint32_t i = 0; i < nkeys; ++i) {
+        b->h_keys[b->plan_slot[i]] = parsed[i];
+        make_aux(parsed[i], &h_aux[b->plan_slot[i]]);
+      }
+      MG_CUDA(cudaMemcpyAsync(b->d_keys, b->h_keys, (size_t)nkeys * (sizeof(KeyDev) + sizeof(mg::KeyAux)),
+                              cudaMemcpyHostToDevice, b->stream));
+      b->in_keys = std::move(parsed);
+      b->plan_reused = true;
+      return MG_OK;
+    }
+  }
+  b->plan_reused = false;
   b->in_keys = std::move(parsed);
   b->in_tables = std::move(tabs);
   b->signature = signature_of(b);
@@ -1520,7 +1583,9 @@ int mg_scan(mg_context* ctx, const mg_table* const* tables, const uint8_t* const
   int rc = mg_batch_set_keys(b, tables, keys, key_lens, nkeys);
   if (rc) return rc;
   MG_CUDA(cudaEventRecord(b->ev_h0, b->stream));  // key H2D was enqueued before this point
-  if ((rc = mg_batch_launch(b, nullptr))) return rc;
+  // A repeated workload (same plan as the previous call) replays the pass
+  // from a CUDA graph; a new one launches directly.
+  if ((rc = b->plan_reused ? mg_batch_launch_graph(b, nullptr) : mg_batch_launch(b, nullptr))) return rc;
   MG_CUDA(cudaMemcpyAsync(b->h_out, b->d_out, (size_t)b->total_cols * 16, cudaMemcpyDeviceToHost,
                           b->stream));
   MG_CUDA(cudaEventRecord(b->ev_h1, b->stream));

@@ -315,3 +315,48 @@ def test_from_chunked_matrix_pads_like_the_reference(scanner, oracle_mod):
     b = scanner.scan_keys(m, [k1])[0][0]
     assert bytes(x ^ y for x, y in zip(a, b)) == want[5 * rb:].tobytes()
     m.close()
+
+
+def test_plan_reuse_restages_keys_and_replans_on_change(scanner, oracle_mod):
+    """A workspace keeps its plan across set_keys calls with the same tables,
+    depths and shape (only the keys are restaged) and replans on any change;
+    every pass stays bit-exact, also through the one-call path, which replays
+    repeated workloads from a CUDA graph."""
+    rb, n = 32, 5000
+    t1, rows1 = make_table(scanner, oracle_mod, n, rb, seed=91)
+    ws = scanner.workspace()
+    for rep in range(3):
+        keys = [oracle_keypair(oracle_mod, 13, (977 * rep + 31 * j) % n, seed=92, i=10 * rep + j)[0] for j in range(3)]
+        ws.set_keys([t1] * 3, keys)
+        ws.launch()
+        assert ws.read() == oracle_mod.scan_fused(keys, rows1, rb)
+        got, _ = scanner.scan_keys(t1, keys)
+        assert got == oracle_mod.scan_fused(keys, rows1, rb)
+    # another depth on the same table
+    keys = [oracle_keypair(oracle_mod, 15, 7 + j, seed=93, i=j)[0] for j in range(3)]
+    ws.set_keys([t1] * 3, keys)
+    ws.launch()
+    assert ws.read() == oracle_mod.scan_fused(keys, rows1, rb)
+    # a table of another shape, possibly at a recycled address
+    t1.close()
+    t2, rows2 = make_table(scanner, oracle_mod, 7001, 64, seed=94)
+    keys = [oracle_keypair(oracle_mod, 13, 100 * j + 1, seed=95, i=j)[0] for j in range(3)]
+    for _ in range(2):
+        ws.set_keys([t2] * 3, keys)
+        ws.launch()
+        assert ws.read() == oracle_mod.scan_fused(keys, rows2, 64)
+        got, _ = scanner.scan_keys(t2, keys)
+        assert got == oracle_mod.scan_fused(keys, rows2, 64)
+    # a delta buffer appears: the pass must fold it
+    t2.delta_reserve(16)
+    idx = np.array([1, 101], np.uint64)
+    diffs = oracle_mod.fill_splitmix(3, 2 * 64, 96).reshape(2, 64)
+    t2.delta_push(idx, diffs)
+    ws.set_keys([t2] * 3, keys)
+    ws.launch()
+    patched = rows2.copy()
+    for i, r in enumerate(idx):
+        patched[r] ^= diffs[i]
+    assert ws.read() == oracle_mod.scan_fused(keys, patched, 64)
+    ws.close()
+    t2.close()
