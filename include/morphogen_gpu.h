@@ -157,7 +157,10 @@ int mg_keygen(uint32_t domain_bits, uint64_t target, const uint8_t root_seed0[16
  * shares are host memory; the copies are inside the call.  timeout_ms == 0
  * waits without a deadline; otherwise MG_ETIMEDOUT is returned if the pass
  * has not finished in time (the pass still completes on the device; the
- * context's internal workspace stays busy until it does).  timing may be NULL. */
+ * context's internal workspace stays busy until it does).  timing may be NULL.
+ * A call with the same tables, key depths and shape as the previous call on
+ * the context reuses its plan and replays the pass from a CUDA graph (the
+ * first such call captures it). */
 int mg_scan(mg_context* ctx, const mg_table* const* tables, const uint8_t* const* keys,
             const size_t* key_lens, uint32_t nkeys, uint8_t* out_shares, uint32_t timeout_ms,
             mg_timing* timing);
