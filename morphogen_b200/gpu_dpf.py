@@ -636,16 +636,24 @@ class GpuScanner:
                 ws.sync(timeout_ms)
             return ws.read()
 
-    def scan_keys(self, db: GpuPageMatrix, keys: Sequence, timeout_ms: int = 0) -> tuple[list[bytes], dict]:
-        """The one-call C entry point mg_scan: host keys in, host shares out."""
+    def scan_keys(self, db, keys: Sequence, timeout_ms: int = 0) -> tuple[list[bytes], dict]:
+        """The one-call C entry point mg_scan: host keys in, host shares out.
+        `db` is one table for every key, or a sequence with one table per key."""
         ka = N.KeyArray([bytes(k) for k in keys])
-        tarr = (C.c_void_p * ka.n)(*([db.handle.value] * ka.n))
-        out = (C.c_uint8 * (db.row_bytes * ka.n))()
+        tabs = list(db) if isinstance(db, (list, tuple)) else [db] * ka.n
+        if len(tabs) != ka.n:
+            raise ValueError("one table per key")
+        tarr = (C.c_void_p * ka.n)(*[t.handle.value for t in tabs])
+        sizes = [t.row_bytes for t in tabs]
+        out = (C.c_uint8 * sum(sizes))()
         tm = N.Timing()
         N.check(N.lib().mg_scan(self._ctx.handle, tarr, ka.ptrs, ka.lens, ka.n, out, timeout_ms, C.byref(tm)))
         raw = bytes(out)
-        rb = db.row_bytes
-        return [raw[i * rb:(i + 1) * rb] for i in range(ka.n)], {
+        res, off = [], 0
+        for rb in sizes:
+            res.append(raw[off:off + rb])
+            off += rb
+        return res, {
             "h2d_ns": tm.h2d_ns, "kernel_ns": tm.kernel_ns, "d2h_ns": tm.d2h_ns, "total_ns": tm.total_ns}
 
     def eval_points(self, key, indices) -> np.ndarray:
