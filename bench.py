@@ -313,6 +313,9 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     host_combine = (lambda sh: combine_shares(sh, device=f"cuda:{local_rank}")) if combiner else (lambda sh: sh)
     ws = scanner.workspace()
     ws.set_kernel(args.kernel)
+    if args.shape:
+        S, Gk = (int(x) for x in args.shape.split(","))
+        ws.set_shape(S, Gk)
     # Correctness gate (outside timing): both servers' shares XOR to the targets.
     ws.set_keys(tables, k1)
     ws.launch()
@@ -589,6 +592,8 @@ def main():
     ap.add_argument("--duration", type=float, default=20.0, help="serve31: seconds of arrivals per rate")
     ap.add_argument("--overload-duration", type=float, default=1.0,
                     help="serve31: seconds of arrivals for rates above capacity")
+    ap.add_argument("--shape", default="",
+                    help="pin the launch shape 'S,G' (tile depth, keys per item) instead of the planner's choice")
     ap.add_argument("--emulate-ranks", default="",
                     help="sharded31 on one GPU: time every rank's row range of R-rank jobs (comma list of R)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "cta", "warp"],
