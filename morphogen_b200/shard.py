@@ -133,3 +133,49 @@ class _null:
 
     def __exit__(self, *a):
         return False
+
+
+class ShardedTable:
+    """One logical table split into contiguous row ranges over several GPUs
+    of this process (the layout of crates/morphogen-gpu-dpf/src/bin/
+    bench_sharded.rs, which gives each GPU thread one page range): every scan
+    runs the same keys on every range at once, one host thread per range,
+    and XORs the range shares into the shares of the whole table.
+
+    scanners: one GpuScanner per range (ranges may share a device)."""
+
+    def __init__(self, scanners, total_rows: int, row_bytes: int, align: int = 1 << 20):
+        from morphogen_b200 import gpu_dpf as G
+
+        self.scanners = list(scanners)
+        self.total_rows, self.row_bytes = total_rows, row_bytes
+        self.spans = [shard_range(total_rows, len(self.scanners), r, align) for r in range(len(self.scanners))]
+        self.tables = [G.GpuPageMatrix.range(sc, first, n, row_bytes)
+                       for sc, (first, n) in zip(self.scanners, self.spans)]
+
+    def fill_splitmix(self, seed: int) -> None:
+        for t in self.tables:
+            t.fill_splitmix(seed)
+
+    def write_rows(self, first_row: int, rows) -> None:
+        """Host rows (n x row_bytes) at logical row first_row, split over the ranges."""
+        data = np.ascontiguousarray(rows, dtype=np.uint8).reshape(-1, self.row_bytes)
+        end = first_row + data.shape[0]
+        for t, (f, n) in zip(self.tables, self.spans):
+            lo, hi = max(first_row, f), min(end, f + n)
+            if lo < hi:
+                t.update_pages(lo - f, data[lo - first_row:hi - first_row])
+
+    def scan(self, keys, timeout_ms: int = 0) -> list[bytes]:
+        """One share per key over the whole logical table."""
+        from concurrent.futures import ThreadPoolExecutor
+
+        kb = [bytes(k) for k in keys]
+        with ThreadPoolExecutor(max_workers=len(self.tables)) as pool:
+            parts = list(pool.map(lambda st: st[0].scan_keys(st[1], kb, timeout_ms)[0],
+                                  zip(self.scanners, self.tables)))
+        return xor_shares(parts)
+
+    def close(self) -> None:
+        for t in self.tables:
+            t.close()

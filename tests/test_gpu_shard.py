@@ -102,3 +102,24 @@ def test_device_combiner_single_rank(scanner, oracle_mod):
     assert out.cpu().numpy().tobytes() == b"".join(ws.read())
     ws.close()
     t.close()
+
+
+def test_in_process_sharded_table(scanner, oracle_mod):
+    """Three ranges scanned concurrently from host threads (here all on one
+    GPU; one per GPU in production) XOR to the whole table's shares, and the
+    two servers' combined shares give the target rows."""
+    from morphogen_b200.shard import ShardedTable
+    rows, rb, d = 300_001, 32, 19
+    whole = oracle_mod.fill_splitmix(0, rows * rb, 51).reshape(rows, rb)
+    st = ShardedTable([scanner] * 3, rows, rb, align=4096)
+    st.write_rows(0, whole)
+    for t, (f, n) in zip(st.tables, st.spans):
+        assert (t.read_rows(0, n).reshape(n, rb) == whole[f:f + n]).all()
+    targets = [5, 150_000, rows - 1]
+    pairs = [oracle_keypair(oracle_mod, d, t, seed=52, i=j) for j, t in enumerate(targets)]
+    a = st.scan([p[0] for p in pairs])
+    b = st.scan([p[1] for p in pairs])
+    assert a == oracle_mod.scan_fused([p[0] for p in pairs], whole, rb)
+    for j, t in enumerate(targets):
+        assert xor_bytes(a[j], b[j]) == whole[t].tobytes()
+    st.close()
