@@ -360,3 +360,24 @@ def test_plan_reuse_restages_keys_and_replans_on_change(scanner, oracle_mod):
     assert ws.read() == oracle_mod.scan_fused(keys, patched, 64)
     ws.close()
     t2.close()
+
+
+@pytest.mark.parametrize("kernel,rb", [("auto", 32), ("cta", 4096), ("warp", 64)])
+def test_empty_table_and_empty_batch(scanner, oracle_mod, kernel, rb):
+    """storage.rs:89-101 allows an empty matrix: every share is zero; an
+    empty batch returns no results (kernel.rs:711-924)."""
+    empty = G.GpuPageMatrix.alloc_empty(scanner, 0, rb)
+    keys = [oracle_keypair(oracle_mod, 10, 3 * j, seed=61, i=j)[0] for j in range(3)]
+    ws = scanner.workspace()
+    ws.set_kernel(kernel)
+    ws.set_keys([empty] * 3, keys)
+    ws.launch()
+    assert ws.read() == [bytes(rb)] * 3
+    ws.close()
+    got, _ = scanner.scan_keys(empty, keys)
+    assert got == [bytes(rb)] * 3
+    assert scanner.scan_batch(empty, []) == []
+    with pytest.raises(G.GpuDpfError):
+        empty.delta_reserve(4)
+        empty.delta_push(np.array([0], np.uint64), np.zeros((1, rb), np.uint8))
+    empty.close()
