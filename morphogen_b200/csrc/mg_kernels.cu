@@ -28,8 +28,10 @@
 
 namespace mg {
 
+// Up to 4 keys per CTA the kernel is held to 80 registers so that three
+// CTAs share an SM (page mode: more bytes in flight per SM).
 template <int G>
-__global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ ScanParams p) {
+__global__ void __launch_bounds__(kThreads, (G <= 4 ? 3 : 2)) scan_kernel(const __grid_constant__ ScanParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KeyDev* s_keys = reinterpret_cast<KeyDev*>(smem_raw);
   uint4* s_mask = reinterpret_cast<uint4*>(smem_raw + G * sizeof(KeyDev));  // [G][2*T]
@@ -115,6 +117,10 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
     const uint4* __restrict__ tbl = sg.table;
     const uint64_t nrows = sg.rows;
     const uint32_t abs0 = d - M;  // tree level of the depth-first roots
+    // Every row of the tile inside the table and every sweep of 8 rows full:
+    // loads need no bounds checks.
+    const bool full_tile = tile_row0 < nrows && nrows - tile_row0 >= (1ull << S) &&
+                           (2 * NR) % (8 * rpi) == 0 && M > 0;
 
     for (uint32_t pi = 0; pi < pairs; ++pi) {
       if (tid < NR) {
@@ -151,7 +157,24 @@ __global__ void __launch_bounds__(kThreads) scan_kernel(const __grid_constant__ 
         }
       }
       __syncthreads();
-      if (scan_thread) {
+      if (scan_thread && full_tile) {
+        const uint4* __restrict__ bp = tbl + (tile_row0 + 2u * pi) * V + lane;
+        for (uint32_t rb = rslot; rb < 2 * NR; rb += 8 * rpi) {
+          uint4 dat[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const uint32_t r = rb + (uint32_t)u * rpi;
+            dat[u] = __ldg(bp + (size_t)(((r >> 1) << M) + (r & 1u)) * V);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const uint32_t r = rb + (uint32_t)u * rpi;
+#pragma unroll
+            for (int k = 0; k < G; ++k)
+              if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat[u], s_mask[(size_t)k * 2 * kThreads + r]);
+          }
+        }
+      } else if (scan_thread) {
         // Eight independent 128-bit loads in flight per thread before any
         // is consumed (wide rows leave one lane position per thread, so
         // this is what keeps enough bytes in flight for HBM).
