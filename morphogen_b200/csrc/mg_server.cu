@@ -41,7 +41,8 @@ struct Request {
   bool done = false;
 };
 
-// Device bytes a key adds to a pass: its device copy, its frontier (17 B per
+// Device bytes a key adds to a pass: its device copy (key and warp-kernel
+// constants, 1200 B), its frontier (17 B per
 // node: at most rows / 2 nodes for tables up to 2^24 rows, rows / 2^8 above,
 // where the planner keeps at least 8 depth-first levels) and partial-row
 // columns for every persistent warp.
@@ -49,7 +50,7 @@ uint64_t key_scratch_bytes(const mg_table* t, int sms) {
   const uint64_t rows = mg_table_rows(t);
   const uint64_t frontier = (rows <= (1ull << 24) ? rows / 2 : rows >> 8) * 17 + 32 * 17;
   const uint64_t partial = (uint64_t)sms * 4 * 8 * (mg_table_row_bytes(t));
-  return 640 + frontier + partial;
+  return 1200 + frontier + partial;
 }
 
 }  // namespace
