@@ -95,6 +95,51 @@ class PirServer:
             pass
 
 
+class ShardedPirServer:
+    """Continuous batching over a table sharded into row ranges across GPUs
+    (morphogen_b200.shard.ShardedTable): one PirServer per range, each
+    request submitted to every range's server (so each GPU folds it into its
+    own next pass) and the range shares XORed when all have answered.  A
+    request's latency is the slowest range's, about 1/N of one GPU's pass."""
+
+    def __init__(self, sharded, slots: int = 2, max_keys_per_pass: int = 0, memory_reserve: int = 1 << 30):
+        self.sharded = sharded
+        self.servers = [PirServer(sc, slots, max_keys_per_pass, memory_reserve) for sc in sharded.scanners]
+        self._next = 0
+        self._ids: dict[int, list[int]] = {}
+        self._lock = threading.Lock()
+
+    def submit(self, keys: Sequence) -> int:
+        """Queue one request: its keys over the sharded table; returns its id."""
+        kb = [bytes(k) for k in keys]
+        rids = [srv.submit([(t, k) for k in kb]) for srv, t in zip(self.servers, self.sharded.tables)]
+        with self._lock:
+            rid = self._next
+            self._next += 1
+            self._ids[rid] = rids
+        return rid
+
+    def wait(self, rid: int, timeout_ms: int = 0) -> tuple[list[bytes], float]:
+        """The request's shares over the whole table and its latency (ms, the
+        slowest range)."""
+        with self._lock:
+            rids = self._ids.pop(rid)
+        parts, lat = [], 0.0
+        for srv, r in zip(self.servers, rids):
+            sh, lt = srv.wait(r, timeout_ms)
+            parts.append(sh)
+            lat = max(lat, lt)
+        from .shard import xor_shares
+        return xor_shares(parts), lat
+
+    def answer(self, keys) -> list[bytes]:
+        return self.wait(self.submit(keys))[0]
+
+    def close(self) -> None:
+        for srv in self.servers:
+            srv.close()
+
+
 def geometric_lookups(rng: np.random.Generator, mean: float = 4.0, lo: int = 1, hi: int = 32) -> int:
     """Lookups per request: geometric on {1, 2, ...} with the given mean, capped to [lo, hi]."""
     return int(min(hi, max(lo, rng.geometric(1.0 / mean))))

@@ -123,3 +123,27 @@ def test_in_process_sharded_table(scanner, oracle_mod):
     for j, t in enumerate(targets):
         assert xor_bytes(a[j], b[j]) == whole[t].tobytes()
     st.close()
+
+
+def test_sharded_serving_loop(scanner, oracle_mod):
+    """Requests folded into passes on every range's serving loop (two ranges
+    on one GPU here) answer exactly what one whole-table scan answers."""
+    from morphogen_b200.server import ShardedPirServer
+    from morphogen_b200.shard import ShardedTable
+    rows, rb, d = 200_003, 32, 18
+    whole = oracle_mod.fill_splitmix(0, rows * rb, 61).reshape(rows, rb)
+    st = ShardedTable([scanner] * 2, rows, rb, align=1024)
+    st.write_rows(0, whole)
+    srv = ShardedPirServer(st, slots=2)
+    reqs = [[oracle_keypair(oracle_mod, d, (7919 * (3 * r + j)) % rows, seed=62, i=3 * r + j)[0] for j in range(3)]
+            for r in range(6)]
+    for s_ in srv.servers:
+        s_.pause()
+    ids = [srv.submit(keys) for keys in reqs]
+    for s_ in srv.servers:
+        s_.resume()
+    for rid, keys in zip(ids, reqs):
+        shares, lat = srv.wait(rid)
+        assert shares == oracle_mod.scan_fused(keys, whole, rb) and lat > 0
+    srv.close()
+    st.close()
