@@ -112,7 +112,14 @@ class ShardedPirServer:
     def submit(self, keys: Sequence) -> int:
         """Queue one request: its keys over the sharded table; returns its id."""
         kb = [bytes(k) for k in keys]
-        rids = [srv.submit([(t, k) for k in kb]) for srv, t in zip(self.servers, self.sharded.tables)]
+        rids: list[int] = []
+        try:
+            for srv, t in zip(self.servers, self.sharded.tables):
+                rids.append(srv.submit([(t, k) for k in kb]))
+        except Exception:
+            for srv, r in zip(self.servers, rids):  # release what was already queued
+                srv.wait(r)
+            raise
         with self._lock:
             rid = self._next
             self._next += 1

@@ -152,6 +152,8 @@ class ShardedTable:
         self.spans = [shard_range(total_rows, len(self.scanners), r, align) for r in range(len(self.scanners))]
         self.tables = [G.GpuPageMatrix.range(sc, first, n, row_bytes)
                        for sc, (first, n) in zip(self.scanners, self.spans)]
+        from concurrent.futures import ThreadPoolExecutor
+        self._pool = ThreadPoolExecutor(max_workers=len(self.tables))
 
     def fill_splitmix(self, seed: int) -> None:
         for t in self.tables:
@@ -168,14 +170,12 @@ class ShardedTable:
 
     def scan(self, keys, timeout_ms: int = 0) -> list[bytes]:
         """One share per key over the whole logical table."""
-        from concurrent.futures import ThreadPoolExecutor
-
         kb = [bytes(k) for k in keys]
-        with ThreadPoolExecutor(max_workers=len(self.tables)) as pool:
-            parts = list(pool.map(lambda st: st[0].scan_keys(st[1], kb, timeout_ms)[0],
-                                  zip(self.scanners, self.tables)))
+        parts = list(self._pool.map(lambda st: st[0].scan_keys(st[1], kb, timeout_ms)[0],
+                                    zip(self.scanners, self.tables)))
         return xor_shares(parts)
 
     def close(self) -> None:
+        self._pool.shutdown(wait=True)
         for t in self.tables:
             t.close()
