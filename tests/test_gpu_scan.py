@@ -381,3 +381,14 @@ def test_empty_table_and_empty_batch(scanner, oracle_mod, kernel, rb):
         empty.delta_reserve(4)
         empty.delta_push(np.array([0], np.uint64), np.zeros((1, rb), np.uint8))
     empty.close()
+
+
+def test_many_key_groups_one_pass(scanner, oracle_mod):
+    """192 keys (64 queries) over one table in one pass: 192 key groups do not
+    divide the persistent warps, so the planner may stride every warp over
+    the tile-major items; bit-exact either way."""
+    rb, nrows, d = 32, 1 << 16, 16
+    db, rows = make_table(scanner, oracle_mod, nrows, rb, seed=71)
+    keys = [oracle_keypair(oracle_mod, d, (40503 * j) % nrows, seed=72, i=j)[0] for j in range(192)]
+    got, _ = scanner.scan_keys(db, keys)
+    assert got == oracle_mod.scan_fused(keys, rows, rb)
