@@ -1039,11 +1039,34 @@ int plan_pass(mg_batch* b) {
   const int Gc = choose_g(Vc, nc, b->eff_G, false);
   const int Gw = choose_g(Vw, nwk, b->eff_G, true);
   std::vector<SegPlan> split;
+  // Warp-kernel segments: warp w keeps key group w % groups, so when the
+  // groups do not divide the persistent warps, nw % groups warps idle.  Above
+  // 1% idle the groups are split into segments whose group counts divide the
+  // warps (largest divisor first, at most 4 segments); every segment is a
+  // separate walk over the table by all warps.  The warp count assumed is two
+  // 8-warp CTAs per SM, what the warp kernel's registers allow.
+  const uint64_t nw_est = (uint64_t)ctx->sms * 2 * mg::kWarps;
+  auto push_warp_groups = [&](const SegPlan& sp, uint32_t g, size_t full) {
+    size_t ng = full / g, at = 0;
+    for (int piece = 0; ng > 0; ++piece) {
+      size_t take = ng;
+      if (piece < 3 && (nw_est % ng) * 100 > nw_est && ng < nw_est)
+        for (size_t c = ng; c >= 1; --c)
+          if (nw_est % c == 0) { take = c; break; }
+      split.push_back(SegPlan{sp.table, sp.d,
+                              std::vector<uint32_t>(sp.keys.begin() + at, sp.keys.begin() + at + take * g), g, true});
+      at += take * g;
+      ng -= take;
+    }
+  };
   for (SegPlan& sp : segs) {
     const int G = sp.warp ? Gw : Gc;
     const uint32_t g = (uint32_t)std::min<size_t>((size_t)G, sp.keys.size());
     const size_t full = sp.keys.size() / g * g;
-    split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin(), sp.keys.begin() + full), g, sp.warp});
+    if (sp.warp && b->eff_S == 0)
+      push_warp_groups(sp, g, full);
+    else
+      split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin(), sp.keys.begin() + full), g, sp.warp});
     if (full < sp.keys.size())
       split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin() + full, sp.keys.end()),
                               (uint32_t)(sp.keys.size() - full), sp.warp});
