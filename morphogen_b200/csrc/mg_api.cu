@@ -1345,6 +1345,7 @@ int mg_batch_autotune(mg_batch* b, uint32_t budget_ms, mg_plan_info* best_info, 
   std::vector<uint8_t> ref, got;
   double best = 1e300;
   Cand best_c = cands[0];
+  std::vector<std::pair<double, size_t>> timed;  // (best ms, candidate index)
   const auto t0 = std::chrono::steady_clock::now();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   MG_CUDA(cudaEventCreate(&e0));
@@ -1386,6 +1387,40 @@ int mg_batch_autotune(mg_batch* b, uint32_t budget_ms, mg_plan_info* best_info, 
     if (ref.empty()) ref = ordered;
     else if (ordered != ref) { rc = fail(MG_ECUDA, "autotune: shape %d/%u/%u changed the shares", c.kind, c.S, c.G); break; }
     if (ms_best < best) { best = ms_best; best_c = c; }
+    timed.push_back({ms_best, ci});
+  }
+  // Confirmation: the three fastest shapes are timed again, alternating, so
+  // that a drift of the clocks during the sweep (power or thermal limits on
+  // HBM-bound passes) does not decide the choice.
+  if (rc == MG_OK && timed.size() > 1) {
+    std::sort(timed.begin(), timed.end());
+    const size_t top = std::min<size_t>(3, timed.size());
+    std::vector<double> again(top, 1e300);
+    for (int round = 0; round < 2 && rc == MG_OK; ++round)
+      for (size_t j = 0; j < top && rc == MG_OK; ++j) {
+        const Cand& c = cands[timed[j].second];
+        b->eff_kind = c.kind;
+        b->eff_S = c.S;
+        b->eff_G = c.G;
+        if (plan_pass(b) != MG_OK) continue;
+        if ((rc = enqueue_pass(b, b->stream, nullptr))) break;
+        for (int r = 0; r < 2 && rc == MG_OK; ++r) {
+          cudaEventRecord(e0, b->stream);
+          rc = enqueue_pass(b, b->stream, nullptr);
+          cudaEventRecord(e1, b->stream);
+          if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(MG_ECUDA, "autotune launch failed"); break; }
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          again[j] = std::min(again[j], (double)ms);
+        }
+      }
+    if (rc == MG_OK) {
+      size_t bj = 0;
+      for (size_t j = 1; j < top; ++j)
+        if (again[j] < again[bj]) bj = j;
+      best = again[bj];
+      best_c = cands[timed[bj].second];
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
