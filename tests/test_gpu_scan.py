@@ -392,3 +392,19 @@ def test_many_key_groups_one_pass(scanner, oracle_mod):
     keys = [oracle_keypair(oracle_mod, d, (40503 * j) % nrows, seed=72, i=j)[0] for j in range(192)]
     got, _ = scanner.scan_keys(db, keys)
     assert got == oracle_mod.scan_fused(keys, rows, rb)
+
+
+def test_prg_peak_and_timers(scanner, oracle_mod):
+    """mg_prg_peak (the ChaCha8 ceiling the bench reports against) gives a
+    plausible rate, and a pass's scan time lies within its total time."""
+    rate = scanner.prg_peak(64)
+    assert 1e9 < rate < 1e12
+    db, rows = make_table(scanner, oracle_mod, 50_000, 32, seed=81)
+    keys = [oracle_keypair(oracle_mod, 16, 7 * j, seed=82, i=j)[0] for j in range(3)]
+    ws = scanner.workspace()
+    ws.set_keys([db] * 3, keys)
+    ws.launch()
+    ws.sync()
+    assert 0 < ws.last_scan_ns() <= ws.last_kernel_ns()
+    assert ws.read() == oracle_mod.scan_fused(keys, rows, 32)
+    ws.close()
