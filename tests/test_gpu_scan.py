@@ -408,3 +408,22 @@ def test_prg_peak_and_timers(scanner, oracle_mod):
     assert 0 < ws.last_scan_ns() <= ws.last_kernel_ns()
     assert ws.read() == oracle_mod.scan_fused(keys, rows, 32)
     ws.close()
+
+
+def test_gpu_matches_recorded_reference_kernel_outputs(scanner, oracle_mod):
+    """Shares recorded from the reference's own CUDA kernel (committed
+    fixtures, make_test_pages pages, depths 8-25): this library's GPU path
+    reproduces every one without the reference present."""
+    import hashlib
+    import json
+    from pathlib import Path
+    data = json.loads((Path(__file__).with_name("golden") / "ref_kernel_pages.json").read_text())
+    for case in data["cases"]:
+        pages = oracle_mod.fill_test_rows(case["pages"], 4096)
+        db = G.GpuPageMatrix.new(scanner, pages, 4096)
+        keys = [bytes.fromhex(k) for k in case["keys"]]
+        got, _ = scanner.scan_keys(db, keys)
+        for j, share in enumerate(got):
+            assert hashlib.sha256(share).hexdigest() == case["sha256"][j]
+            assert share[:64].hex() == case["head"][j] and share[-64:].hex() == case["tail"][j]
+        db.close()
