@@ -8,13 +8,25 @@ Default workload (one step = one scan pass answering one query):
 
 `value` is scanned GB/s (table bytes per pass / device time per pass, keys
 resident); `e2e` is the same metric through the one-call C entry point
-mg_scan with host keys in and host shares out.  The roofline object reports
-the dominant kernel (the fused subtree-expansion + scan kernel) against the
-measured HBM copy bandwidth, and `alu` reports it against the ChaCha8 PRG
-ceiling measured in the same run (the binding resource on this workload).
+mg_scan with host keys in and host shares out.  `roofline` reports the
+dominant kernel against its binding resource: the integer ALU pipe running
+ChaCha8 (node expansions per second against the PRG-only ceiling measured
+in the same run), with the HBM fraction beside it (`roofline.hbm`).
+
+On one GPU the default run adds, in the same JSON line:
+  c1       the full 2^20 rows x 256 B configuration (3 x 20-bit keys),
+           autotuned, passes replayed from a CUDA graph;
+  batched  Q = 1 and 8 queries (3 keys each) per pass over the 2^31 x 32 B
+           table, launch shape autotuned on a 2^26-row window of the same
+           table and kept only if faster on the full table, graph replay;
+  pages    the reference's own layout (16,817,159 pages x 4096 B, 25-bit
+           keys): this library's pass against the reference's
+           fused_batch_pir_kernel_1 compiled for sm_100a, on the same table
+           and keys, shares compared.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                   [--workload plain31|plain20|batched31 --queries Q|sharded31|pages|mixed|serve31]
+                  [--no-extras] [--no-cpu]
 
 Multi-GPU (torchrun, one process per GPU): by default every rank serves an
 independent replica of the table (no collective; weak scaling), timing is the
@@ -62,8 +74,10 @@ WORKLOADS = {
 }
 KEYS_PER_QUERY = 3
 SEED = 0
-CPU_SAMPLE_BYTES = 8 << 30     # aligned window timed on the host cores (cpu_baseline): 2^28 rows of 32 B
+CPU_SAMPLE_BYTES = 4 << 30     # aligned window timed on the host cores (cpu_baseline): 2^27 rows of 32 B
 REF_SAMPLE_BYTES = 1 << 30     # per-step sample of the reference arm: 2^25 rows of 32 B
+PROXY_ROWS = 1 << 26           # window of the 2^31-row table the batched shapes are autotuned on
+PAGES = 16_817_159             # the reference's mainnet page matrix (docs/benchmarks/...-h100-matrix.csv)
 
 
 def measured_peaks() -> dict:
@@ -155,25 +169,66 @@ class ClockSampler:
         return res
 
 
-def cpu_scan_sample(keys, rows_total: int, row_bytes: int, sample_rows: int, reps: int = 1):
+def cpu_info() -> dict:
+    """Host CPU model, logical CPUs and physical cores (the baseline's `cores`
+    is the OpenMP thread count actually used)."""
+    model = "unknown"
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    physical = None
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False)
+    except Exception:
+        pass
+    return {"cpu_model": model, "logical_cpus": os.cpu_count(), "physical_cores": physical}
+
+
+def cpu_scan_sample(keys, rows_total: int, row_bytes: int, sample_rows: int, reps: int = 1,
+                    avx512: bool = True, base: int | None = None) -> dict:
     """Time the oracle (the restated reference CPU scan: eval_fused_3dpf_cpu
-    with scalar ChaCha8, OpenMP over all host threads) on an aligned window of
-    the table.  Returns (GB/s per rep list, threads, description)."""
+    with scalar ChaCha8, OpenMP over all host threads) on an aligned window
+    of the table.  avx512: the AND/XOR loop in 512-bit registers, eight rows
+    per step (the reference server's AVX-512 scan shape, scan.rs:719-895) when
+    the host has AVX-512F.  Returns per-rep seconds and GB/s with the host
+    description."""
     import oracle
     oracle.build()
-    base = (rows_total // 2) // sample_rows * sample_rows
+    use_avx = avx512 and oracle.avx512_available()
+    if base is None:
+        base = (rows_total // 2) // sample_rows * sample_rows
     host = oracle.fill_splitmix(base * row_bytes, sample_rows * row_bytes, SEED)
     kb = [bytes(k) for k in keys]
     nthreads = os.cpu_count() or 1
-    rates = []
+    secs = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        oracle.scan_fused(kb, host, row_bytes, row_base=base, nthreads=nthreads)
-        dt = time.perf_counter() - t0
-        rates.append(sample_rows * row_bytes / dt / 1e9)
+        oracle.scan_fused(kb, host, row_bytes, row_base=base, nthreads=nthreads, avx512=use_avx)
+        secs.append(time.perf_counter() - t0)
+    window = sample_rows * row_bytes
+    rates = [window / t / 1e9 for t in secs]
+    variant = ("AND/XOR in AVX-512 registers, 8 rows per step (scan.rs:719-895 shape); scalar ChaCha8"
+               if use_avx else "scalar AND/XOR (kernel.rs:1243-1256); scalar ChaCha8")
     desc = (f"{len(kb)} keys over the aligned window of {sample_rows} rows starting at row {base} "
-            f"({sample_rows * row_bytes / 2**30:.1f} GiB); GB/s of that window")
-    return rates, nthreads, desc
+            f"({window / 2**30:.2f} GiB); GB/s of that window")
+    return {"rates": rates, "secs": secs, "threads": nthreads, "window_bytes": window, "variant": variant,
+            "avx512": use_avx, "desc": desc, **cpu_info()}
+
+
+def cpu_baseline_obj(c: dict, scalar: dict | None = None) -> dict:
+    v = sum(c["rates"]) / len(c["rates"])
+    o = {"value": round(v, 4), "unit": "GB/s", "cores": c["threads"], "kind": "port", "sample": c["desc"],
+         "variant": c["variant"], "per_rep_s": [round(x, 4) for x in c["secs"]], "window_bytes": c["window_bytes"],
+         "cpu_model": c["cpu_model"], "logical_cpus": c["logical_cpus"], "physical_cores": c["physical_cores"]}
+    if scalar:
+        o["scalar_variant"] = {"value": round(sum(scalar["rates"]) / len(scalar["rates"]), 4),
+                               "per_rep_s": [round(x, 4) for x in scalar["secs"]], "variant": scalar["variant"]}
+    return o
 
 
 def run_reference(args, rank: int, world: int):
@@ -186,10 +241,12 @@ def run_reference(args, rank: int, world: int):
     nq = int(str(args.queries).split(",")[0]) if args.workload == "batched31" else 1
     k0, _, _ = seeded_keys(wl["d"], wl["rows"], nq)
     sample = min(REF_SAMPLE_BYTES // wl["row_bytes"], wl["rows"])
-    _, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.warmup)
-    rates, threads, desc = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.steps)
-    v = sum(rates) / len(rates)
+    cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.warmup)
+    c = cpu_scan_sample(k0, wl["rows"], wl["row_bytes"], sample, reps=args.steps)
+    v = sum(c["rates"]) / len(c["rates"])
     gb_pass = wl["rows"] * wl["row_bytes"] / 1e9
+    cb = cpu_baseline_obj(c)
+    cb["sample"] += "; ms_per_step extrapolates the window's time to the full table"
     line = {
         "impl": "reference", "metric": "scanned GB/s", "value": round(v, 4), "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -197,8 +254,7 @@ def run_reference(args, rank: int, world: int):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": wl["name"], "queries_per_pass": nq, "keys": nq * KEYS_PER_QUERY,
                    "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": desc + "; ms_per_step extrapolates to the full table"},
+        "cpu_baseline": cb,
         "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -299,23 +355,33 @@ def target_rows(table, targets, rb: int, dist, local_rank: int) -> list[bytes]:
     return [buf[j].astype(np.uint8).tobytes() for j in range(len(targets))]
 
 
-def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist, combiner=None):
+def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist, combiner=None,
+            graph=None, autotune=None, steps=None, warmup=None, pin=None):
     """One workload point: correctness gate, optional autotune, K timed device
     passes (CUDA events on the launching stream), e2e passes through mg_scan.
     tables[i] is the table of key i.  With a ShardCombiner every pass is
     followed by the XOR-combine of the ranks' shares (tables are row ranges of
-    one logical table).  Returns the fields of the JSON line."""
+    one logical table).  graph / autotune / steps / warmup override the
+    command line for this point; pin = (kernel, subtree_bits, keys_per_item)
+    fixes the launch shape.  Returns the fields of the JSON line."""
     import torch
 
     from morphogen_b200.shard import combine_shares
 
+    graph = args.graph if graph is None else graph
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     nkeys = len(k0)
     host_combine = (lambda sh: combine_shares(sh, device=f"cuda:{local_rank}")) if combiner else (lambda sh: sh)
     ws = scanner.workspace()
-    ws.set_kernel(args.kernel)
-    if args.shape:
-        S, Gk = (int(x) for x in args.shape.split(","))
-        ws.set_shape(S, Gk)
+    if pin:
+        ws.set_kernel(pin[0])
+        ws.set_shape(pin[1], pin[2])
+    else:
+        ws.set_kernel(args.kernel)
+        if args.shape:
+            S, Gk = (int(x) for x in args.shape.split(","))
+            ws.set_shape(S, Gk)
     # Correctness gate (outside timing): both servers' shares XOR to the targets.
     ws.set_keys(tables, k1)
     ws.launch()
@@ -332,11 +398,11 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     if not verified:
         raise SystemExit("bench: shares do not reconstruct the target rows")
     tuned = None
-    budget = args.autotune
+    budget = args.autotune if autotune is None else autotune
     if budget < 0:
         ws.launch()
         ws.sync()
-        budget = 5000 if ws.last_kernel_ns() < 20e6 and args.kernel == "auto" else 0
+        budget = 5000 if ws.last_kernel_ns() < 20e6 and args.kernel == "auto" and not pin else 0
     if budget > 0:
         tuned = ws.autotune(budget)
         ws.launch()
@@ -348,13 +414,13 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
 
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
-    for _ in range(args.warmup):
-        ws.launch(stream=sh, graph=args.graph)
+    for _ in range(warmup):
+        ws.launch(stream=sh, graph=graph)
         if combiner:
             combiner.combine(ws, stream)
     torch.cuda.synchronize()
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     scan_ns = []
     clocks = ClockSampler(local_rank)
     if dist:
@@ -364,9 +430,9 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
-    for i in range(args.steps):
+    for i in range(steps):
         ev[i][0].record(stream)
-        ws.launch(stream=sh, graph=args.graph)
+        ws.launch(stream=sh, graph=graph)
         if combiner:
             combiner.combine(ws, stream)
         ev[i][1].record(stream)
@@ -382,16 +448,16 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
         tt = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         total_ms = float(tt.item())
-    ms_per_step = total_ms / args.steps
+    ms_per_step = total_ms / steps
 
     # e2e: host keys in, host shares out, through the one-call C entry point
     # mg_scan (GpuScanner::scan; repeated passes replay from a CUDA graph).
     e2e_ms = []
-    for i in range(args.warmup + args.steps):
+    for i in range(warmup + steps):
         t0 = time.perf_counter()
         shares = host_combine(scanner.scan_keys(tables, k0)[0])
         dt = (time.perf_counter() - t0) * 1e3
-        if i >= args.warmup:
+        if i >= warmup:
             e2e_ms.append(dt)
     if shares != s0:
         raise SystemExit("bench: e2e shares differ")
@@ -402,7 +468,179 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
         e2e_per = float(tt.item())
     ws.close()
     return dict(plan=plan, verified=verified, ms_per_step=ms_per_step, step_ms=step_ms, e2e_ms=e2e_ms,
-                e2e_per=e2e_per, scan_avg_s=sum(scan_ns) / len(scan_ns) * 1e-9, clocks=clk)
+                e2e_per=e2e_per, scan_avg_s=sum(scan_ns) / len(scan_ns) * 1e-9, clocks=clk, shares0=s0_local,
+                steps=steps, warmup=warmup, graph=bool(graph))
+
+
+def pct3(xs) -> dict:
+    a = np.array(xs)
+    return {"p50": round(float(np.percentile(a, 50)), 3), "p95": round(float(np.percentile(a, 95)), 3),
+            "p99": round(float(np.percentile(a, 99)), 3)}
+
+
+def rooflines(bytes_scanned: int, nodes: int, seconds: float, prg_peak: float, hbm_peak: float, peaks: dict,
+              traffic) -> dict:
+    """The dominant kernel against both of its bounds.  `bound` names the
+    binding one (the larger fraction); the other sits beside it."""
+    a_nodes = nodes / seconds
+    a_hbm = bytes_scanned / seconds / 1e9
+    alu = {"achieved": round(a_nodes / 1e9, 3), "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
+           "frac": round(a_nodes / prg_peak, 4),
+           "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run (of measured)"}
+    hbm = {"achieved": round(a_hbm, 2), "peak": hbm_peak, "unit": "GB/s", "frac": round(a_hbm / hbm_peak, 4),
+           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "fallback" not in peaks
+           else "fallback 6650 GB/s (of fallback)"}
+    if alu["frac"] >= hbm["frac"]:
+        return {"bound": "alu", "what": "int32 ALU pipe (ChaCha8 node expansions)", **alu, "traffic": traffic,
+                "hbm": hbm}
+    return {"bound": "hbm", **hbm, "traffic": traffic, "alu": alu}
+
+
+def traffic_for(traffic_rec: dict, kernel_kind: int, bytes_scanned: int):
+    """DRAM read + write bytes per launch: the ratio ncu measured on a smaller
+    capture of the same kernel, scaled by the rows scanned."""
+    rec = traffic_rec.get("scan_warp_kernel" if kernel_kind == 2 else "scan_kernel", {})
+    if not rec.get("table_bytes"):
+        return None
+    return round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_scanned)
+
+
+def run_c1(args, scanner, prg_peak, hbm_peak, peaks, traffic_rec, local_rank) -> dict:
+    """The plain single query at 2^20 rows x 256 B (3 x 20-bit keys):
+    autotuned shape, passes replayed from a CUDA graph."""
+    from morphogen_b200 import gpu_dpf as G
+    wl = WORKLOADS["plain20"]
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    table = G.GpuPageMatrix.from_seed(scanner, rows, rb, seed=SEED)
+    k0, k1, targets = seeded_keys(d, rows, 1)
+    m = measure(args, scanner, [table] * 3, k0, k1, target_rows(table, targets, rb, None, local_rank), 1,
+                local_rank, None, graph=True, autotune=5000, steps=200, warmup=20)
+    nodes = 3 * expansions(0, rows, d)
+    bytes_pass = rows * rb
+    out = {
+        "workload": wl["name"], "keys": 3, "steps": m["steps"], "warmup": m["warmup"], "cuda_graph": True,
+        "plan": m["plan"], "ms_per_step": round(m["ms_per_step"], 4),
+        "GBps": round(bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9, 2),
+        "queries_per_s": round(1e3 / m["ms_per_step"], 1),
+        "latency_ms": pct3(m["step_ms"]),
+        "e2e": {"value": round(bytes_pass / (m["e2e_per"] * 1e-3) / 1e9, 2), "unit": "GB/s",
+                "ms": round(m["e2e_per"], 4), **{f"{k}_ms": v for k, v in pct3(m["e2e_ms"]).items()}},
+        "roofline": rooflines(bytes_pass, nodes, m["scan_avg_s"], prg_peak, hbm_peak, peaks,
+                              traffic_for(traffic_rec, m["plan"].get("kernel"), bytes_pass)),
+        "roofline_note": "a replayed pass is timed as a whole (frontier chain, scan and reduction kernels)",
+        "verified": m["verified"], "clocks": m["clocks"], "l2": "table (268 MB) larger than L2 (126 MB)",
+    }
+    if not args.no_cpu:
+        import oracle
+        c = cpu_scan_sample(k0, rows, rb, rows, reps=3, base=0)
+        sc = cpu_scan_sample(k0, rows, rb, rows, reps=3, base=0, avx512=False)
+        out["cpu_baseline"] = cpu_baseline_obj(c, sc)
+        host = oracle.fill_splitmix(0, bytes_pass, SEED)
+        out["cpu_shares_equal"] = oracle.scan_fused([bytes(k) for k in k0], host, rb, avx512=c["avx512"]) == \
+            m["shares0"]
+    table.close()
+    return out
+
+
+def run_batched(args, scanner, table, prg_peak, hbm_peak, peaks, local_rank, qlist=(1, 8)) -> dict:
+    """Q queries (3 keys each) per pass over the 2^31 x 32 B table.  The
+    autotuner runs on a 2^26-row window of the same table with the same keys
+    (a full-size candidate pass takes Q x 0.18 s); its shape is kept only if
+    it is faster than the planner's on the full table.  Timed passes replay a
+    CUDA graph."""
+    from morphogen_b200 import gpu_dpf as G
+    wl = WORKLOADS["plain31"]
+    rows, rb, d = wl["rows"], wl["row_bytes"], wl["d"]
+    proxy = G.GpuPageMatrix.from_seed(scanner, PROXY_ROWS, rb, seed=SEED)
+    kinds = {1: "cta", 2: "warp"}
+    out = {"workload": wl["name"], "tuning": f"autotuned on rows [0, 2^26) of the same table (5 s budget)",
+           "points": []}
+    for q in qlist:
+        k0, k1, targets = seeded_keys(d, rows, q, seed=SEED + 100 + q)
+        nk = len(k0)
+        wp = scanner.workspace()
+        wp.set_keys([proxy] * nk, k0)
+        tuned = wp.autotune(5000)
+        wp.close()
+        cand = (kinds[tuned["kernel"]], tuned["subtree_bits"], tuned["keys_per_cta"])
+        # planner's shape vs the proxy's, one full-size pass each
+        timings = {}
+        for name, pin in (("planner", None), ("autotuned", cand)):
+            ws = scanner.workspace()
+            if pin:
+                ws.set_kernel(pin[0])
+                ws.set_shape(pin[1], pin[2])
+            ws.set_keys([table] * nk, k0)
+            ws.launch()
+            ws.sync()
+            timings[name] = ws.last_kernel_ns() / 1e6
+            ws.close()
+        pin = cand if timings["autotuned"] < timings["planner"] else None
+        steps, warmup = (5, 2) if q == 1 else (3, 1)
+        m = measure(args, scanner, [table] * nk, k0, k1, target_rows(table, targets, rb, None, local_rank), 1,
+                    local_rank, None, graph=True, autotune=0, steps=steps, warmup=warmup, pin=pin)
+        nodes = nk * expansions(0, rows, d)
+        bytes_pass = rows * rb
+        out["points"].append({
+            "queries_per_pass": q, "keys": nk, "steps": steps, "warmup": warmup, "cuda_graph": True,
+            "plan": m["plan"], "shape": "autotuned" if pin else "planner",
+            "full_size_candidate_ms": {k: round(v, 2) for k, v in timings.items()},
+            "ms_per_pass": round(m["ms_per_step"], 2),
+            "queries_per_s": round(q / (m["ms_per_step"] * 1e-3), 3),
+            "per_key_GBps": round(nk * bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9, 1),
+            "latency_ms": pct3(m["step_ms"]),
+            "e2e_queries_per_s": round(q / (m["e2e_per"] * 1e-3), 3),
+            "alu_frac": round(nodes / m["scan_avg_s"] / prg_peak, 4),
+            "hbm_frac": round(bytes_pass / m["scan_avg_s"] / 1e9 / hbm_peak, 4),
+            "verified": m["verified"], "clocks": m["clocks"]})
+    proxy.close()
+    base = out["points"][0]["queries_per_s"]
+    for pt in out["points"]:
+        pt["speedup_vs_q1"] = round(pt["queries_per_s"] / base, 3)
+    return out
+
+
+def run_pages(args, scanner, hbm_peak, peaks, traffic_rec, local_rank, pages: int = PAGES) -> dict:
+    """Page mode, the reference's own layout: this library's pass against the
+    reference's fused_batch_pir_kernel_1 (the server's single-query kernel,
+    compiled unmodified for sm_100a into oracle/_ref and launched with the
+    reference's recipe) on the same table and keys, shares compared."""
+    from morphogen_b200 import gpu_dpf as G
+    rb, d = 4096, 25
+    table = G.GpuPageMatrix.from_seed(scanner, pages, rb, seed=SEED)
+    k0, k1, targets = seeded_keys(d, pages, 1)
+    m = measure(args, scanner, [table] * 3, k0, k1, target_rows(table, targets, rb, None, local_rank), 1,
+                local_rank, None, graph=True, autotune=5000, steps=20, warmup=5)
+    bytes_pass = pages * rb
+    ours_best = min(m["step_ms"])
+    out = {
+        "workload": f"page mode: {pages:,} pages x 4096 B ({bytes_pass / 1e9:.1f} GB), 3 x 25-bit keys",
+        "steps": m["steps"], "warmup": m["warmup"], "cuda_graph": True, "plan": m["plan"],
+        "ms_per_step": round(m["ms_per_step"], 3), "best_ms": round(ours_best, 3),
+        "GBps": round(bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9, 1),
+        "latency_ms": pct3(m["step_ms"]),
+        "e2e": {"value": round(bytes_pass / (m["e2e_per"] * 1e-3) / 1e9, 1), "unit": "GB/s"},
+        "roofline": rooflines(bytes_pass, 3 * expansions(0, pages, d), m["scan_avg_s"], 1e30, hbm_peak, peaks,
+                              traffic_for(traffic_rec, m["plan"].get("kernel"), bytes_pass)),
+        "verified": m["verified"], "clocks": m["clocks"],
+    }
+    out["roofline"].pop("alu", None)
+    try:
+        import oracle
+        if not oracle.ref_available():
+            raise RuntimeError("oracle/_ref/libmg_refkernels.so was not built")
+        shares, ref_best = oracle.ref_scan(0, [bytes(k) for k in k0], table.device_ptr(), pages, reps=5)
+        out["reference_kernel"] = {
+            "kernel": "fused_batch_pir_kernel_1 (cuda/fused_kernel.cu), compiled for sm_100a, reference launch "
+                      "recipe (kernel.rs:293-303,774-787)",
+            "best_ms": round(ref_best, 3), "GBps": round(bytes_pass / (ref_best * 1e-3) / 1e9, 1),
+            "reps": 5, "shares_equal": shares == m["shares0"],
+            "speedup_mean_vs_ref_best": round(ref_best / m["ms_per_step"], 3),
+            "speedup_best_vs_best": round(ref_best / ours_best, 3)}
+    except Exception as e:  # the baseline leg only; this library's numbers stand
+        out["reference_kernel"] = {"unavailable": str(e)}
+    table.close()
+    return out
 
 
 def run_gpu(args, rank: int, world: int, local_rank: int):
@@ -437,7 +675,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     except (OSError, ValueError):
         traffic_rec = {}
     bytes_pass = rows * rb
-    cpu = None
+    extras = world == 1 and args.workload == "plain31" and not args.no_extras
+    line = None
     for nq in qlist:
         k0, k1, targets = seeded_keys(d, rows, nq)
         nkeys = len(k0)
@@ -450,22 +689,15 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         copies = 1 if sharded else world
         value = copies * bytes_pass / (m["ms_per_step"] * 1e-3) / 1e9
         e2e_value = copies * bytes_pass / (m["e2e_per"] * 1e-3) / 1e9
-        # Rooflines of the dominant kernel (this rank's launch); DRAM traffic
-        # per launch is the ratio ncu measured on a smaller capture of the
-        # same kernel, scaled.
+        # Rooflines of the dominant kernel (this rank's launch): node
+        # expansions and bytes of the launch over its CUDA-event time.
         local_bytes = n_local * rb
-        achieved_hbm = local_bytes / m["scan_avg_s"] / 1e9
-        rec = traffic_rec.get("scan_warp_kernel" if plan.get("kernel") == 2 else "scan_kernel", {})
-        traffic = (round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * local_bytes)
-                   if rec.get("table_bytes") and nkeys == 3 else None)
         nodes = nkeys * expansions(first, n_local, d)
-        achieved_nodes = nodes / m["scan_avg_s"]
+        roof = rooflines(local_bytes, nodes, m["scan_avg_s"], prg_peak, hbm_peak, peaks,
+                         traffic_for(traffic_rec, plan.get("kernel"), local_bytes) if nkeys == 3 else None)
+        roof["timed"] = "frontier chain + scan kernel of each pass (CUDA events before the reduction)"
         if rank != 0:
             continue
-        if cpu is None and world == 1 and not args.no_cpu:
-            rates, threads, desc = cpu_scan_sample(k0[:3], rows, rb, min(CPU_SAMPLE_BYTES // rb, rows))
-            cpu = {"value": round(rates[0], 4), "unit": "GB/s", "cores": threads, "kind": "port", "sample": desc}
-        pct = lambda xs, q: float(np.percentile(np.array(xs), q))  # noqa: E731
         line = {
             "metric": "scanned GB/s", "value": round(value, 2), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(m["ms_per_step"], 3),
@@ -477,27 +709,29 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                        "rows_per_rank": n_local,
                        "cuda_graph": bool(args.graph), "plan": plan,
                        "l2": "inputs larger than L2" if bytes_pass > 126e6 else "table fits L2"},
-            "latency_ms": {"p50": round(pct(m["step_ms"], 50), 3), "p95": round(pct(m["step_ms"], 95), 3),
-                           "p99": round(pct(m["step_ms"], 99), 3), "e2e_p50": round(pct(m["e2e_ms"], 50), 3), "e2e_p95": round(pct(m["e2e_ms"], 95), 3),
-                           "e2e_p99": round(pct(m["e2e_ms"], 99), 3)},
+            "latency_ms": {**pct3(m["step_ms"]), **{f"e2e_{k}": v for k, v in pct3(m["e2e_ms"]).items()}},
             "queries_per_s": round(copies * nq / (m["ms_per_step"] * 1e-3), 3),
             "per_key_GBps": round(value * nkeys, 2),
             "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": sum(len(bytes(k)) for k in k0), "d2h_bytes_per_step": nkeys * rb},
-            "roofline": {"bound": "hbm", "achieved": round(achieved_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
-                         "frac": round(achieved_hbm / hbm_peak, 4), "traffic": traffic,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"
-                         if "fallback" not in peaks else "fallback 6650 GB/s"},
-            "alu": {"bound": "int32 ALU pipe (ChaCha8)", "achieved": round(achieved_nodes / 1e9, 3),
-                    "peak": round(prg_peak / 1e9, 3), "unit": "G node expansions/s",
-                    "frac": round(achieved_nodes / prg_peak, 4),
-                    "peak_source": "mg_prg_peak: device ChaCha8 PRG alone, measured in this run"},
+            "roofline": roof,
             "gpu_launches": plan["kernels"] * args.steps,
             "clocks": m["clocks"],
             "verified": m["verified"],
         }
-        if cpu:
-            line["cpu_baseline"] = cpu
+        if world == 1 and not args.no_cpu:
+            sample = min(CPU_SAMPLE_BYTES // rb, rows)
+            c = cpu_scan_sample(k0[:3], rows, rb, sample)
+            sc = cpu_scan_sample(k0[:3], rows, rb, sample, avx512=False) if c["avx512"] else None
+            line["cpu_baseline"] = cpu_baseline_obj(c, sc)
+        if len(qlist) > 1:
+            print(json.dumps(line), flush=True)
+    if extras and rank == 0:
+        line["batched"] = run_batched(args, scanner, table, prg_peak, hbm_peak, peaks, local_rank)
+        table.close()
+        line["c1"] = run_c1(args, scanner, prg_peak, hbm_peak, peaks, traffic_rec, local_rank)
+        line["pages"] = run_pages(args, scanner, hbm_peak, peaks, traffic_rec, local_rank)
+    if rank == 0 and line is not None and len(qlist) == 1:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -585,6 +819,8 @@ def main():
     ap.add_argument("--queries", default="1", help="batched31: queries per pass, or a comma list to sweep")
     ap.add_argument("--graph", action="store_true", help="replay the timed passes from a CUDA graph")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain31 on one GPU: skip the c1 / batched / pages points of the default line")
     ap.add_argument("--autotune", type=int, default=-1,
                     help="autotuner budget in ms before timing (-1: 5000 when a pass is under 20 ms, else off)")
     ap.add_argument("--rates", default="0.25,0.5,1,2,100",

@@ -222,7 +222,10 @@ int mg_eval_points(mg_context* ctx, const uint8_t* key, size_t key_len, const ui
  * mg_server_resume. */
 typedef struct {
   uint32_t slots;             /* concurrent passes (default 2) */
-  uint32_t max_keys_per_pass; /* 0 = no cap */
+  uint32_t max_keys_per_pass; /* 0 = latency-aware: a pass is closed once its
+                                 estimated device time (tree nodes of its keys
+                                 over the rate measured on completed passes)
+                                 reaches 50 ms; always at least one request */
   uint64_t memory_reserve;    /* device bytes kept free (default 1 GiB) */
 } mg_server_config;
 
@@ -239,6 +242,9 @@ typedef struct {
 
 typedef struct mg_server mg_server;
 int mg_server_create(mg_context* ctx, const mg_server_config* cfg, mg_server** out);
+/* Completes the passes already on the GPU, answers requests not yet
+ * dispatched with MG_EBUSY (threads blocked in mg_server_wait wake up and
+ * return it), waits for those threads to leave, then frees the server. */
 int mg_server_destroy(mg_server* server);
 /* Queue one request (its keys, key i over tables[i]); returns its id. */
 int mg_server_submit(mg_server* server, const mg_table* const* tables, const uint8_t* const* keys,
@@ -265,7 +271,9 @@ int mg_server_reset_stats(mg_server* server);
  * nkeys * row_bytes of device memory, share i at offset i * row_bytes.  Keys
  * are host bytes in the wire format and must all have the same domain_bits.
  * The work is enqueued on `stream` (a cudaStream_t, NULL = legacy default)
- * and the shares are valid once the stream reaches it.
+ * and the shares are valid once the stream reaches it.  The parsed keys go
+ * to the device by value inside kernel parameters: the call does not wait
+ * for the stream, and the caller may reuse its key buffers on return.
  *
  * Limits: nkeys <= MG_NOALLOC_MAX_KEYS, and nkeys * 624 bytes of keys plus
  * (persistent CTAs) x nkeys x row_bytes bytes of partial rows must fit the

@@ -153,9 +153,6 @@ struct mg_context {
   int sms = 0;
   size_t smem_optin = 0;
   std::mutex mu;              // serialises the one-call path (mg_scan)
-  std::mutex attr_mu;         // kernel attribute setup
-  size_t prepared_smem[9] = {0};
-  size_t prepared_warp[5][6] = {};
   mg_batch* internal = nullptr;
   std::mutex tune_mu;  // tuned launch shapes per workload signature
   std::map<std::string, std::array<uint32_t, 3>> tuned;  // {kind, subtree_bits, keys_per_item}
@@ -264,26 +261,18 @@ int set_device(const T* obj) {
   return MG_OK;
 }
 
+// The kernels' shared-memory limits are process-wide per device; the
+// launchers keep one high-water mark for every caller (scan_prepare /
+// warp_prepare only raise it), so nothing is cached per context.
 int prepare_g(mg_context* ctx, int G, size_t smem) {
-  std::lock_guard<std::mutex> lk(ctx->attr_mu);
-  if (ctx->prepared_smem[G] >= smem) return MG_OK;
+  (void)ctx;
   MG_CUDA(mg::scan_prepare(G, smem));
-  ctx->prepared_smem[G] = smem;
   return MG_OK;
 }
 
-int vt_index(uint32_t VT) {
-  int i = 0;
-  while ((1u << i) < VT) ++i;
-  return i;  // 1,2,4,...,32 -> 0..5
-}
-
 int prepare_warp(mg_context* ctx, int G, uint32_t VT, size_t smem) {
-  std::lock_guard<std::mutex> lk(ctx->attr_mu);
-  size_t& have = ctx->prepared_warp[G][vt_index(VT)];
-  if (have >= smem) return MG_OK;
+  (void)ctx;
   MG_CUDA(mg::warp_prepare(G, VT, smem));
-  have = smem;
   return MG_OK;
 }
 
@@ -378,7 +367,6 @@ void shape_for(uint32_t d, uint32_t S_target, uint32_t& S, uint32_t& U, uint32_t
   M = S - U;
 }
 
-uint64_t ceil_shift(uint64_t x, uint32_t s) { return s >= 64 ? (x ? 1 : 0) : (x + (1ull << s) - 1) >> s; }
 
 // Tree nodes 2^s leaves wide that meet the table's rows [first, first + rows):
 // their first level index and their count.

@@ -11,6 +11,9 @@ namespace mg {
 
 size_t scan_smem_bytes(int G, uint32_t slots);
 bool scan_g_supported(int G);
+// Raise (never lower) the kernel's dynamic shared memory limit on the current
+// device to at least smem.  The limit is process-wide per device and kernel,
+// so every caller goes through this one record (scan_prepare / warp_prepare).
 cudaError_t scan_prepare(int G, size_t smem);
 int scan_occupancy(int G, size_t smem);
 cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st);

@@ -20,7 +20,10 @@
 // 64-bit XOR atomics into the zeroed shares.  XOR is
 // associative and commutative, so the shares are bit-exact whatever the
 // schedule.  The kernels contain no waits on other CTAs or on the host.
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <utility>
 
 #include "mg_device.cuh"
 #include "mg_internal.h"
@@ -765,6 +768,29 @@ __global__ void __launch_bounds__(256) prg_peak_kernel(uint32_t* __restrict__ ou
 
 // ---- host-side launchers --------------------------------------------------
 
+// The dynamic shared memory limit of a kernel (cudaFuncAttributeMax-
+// DynamicSharedMemorySize) belongs to the kernel function on its device, for
+// the whole process: every context, workspace and the allocation-free entry
+// point see the same value.  It is therefore kept here as one high-water mark
+// per (device, kernel) under one mutex and only ever raised, so that a caller
+// preparing a small launch can never lower the limit under another caller's
+// larger launch.
+namespace {
+std::mutex g_smem_mu;
+std::map<std::pair<int, const void*>, size_t> g_smem_limit;
+
+cudaError_t raise_smem_limit(const void* fn, size_t smem) {
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev)) return e;
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  size_t& have = g_smem_limit[{dev, fn}];
+  if (have >= smem) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) have = smem;
+  return e;
+}
+}  // namespace
+
 cudaError_t prg_peak_shape(int sms, uint32_t* blocks, uint32_t* threads) {
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, prg_peak_kernel, 256, 0);
@@ -792,7 +818,7 @@ static cudaError_t launch_scan_t(const ScanParams& p, uint32_t grid, size_t smem
 
 template <int G>
 static cudaError_t prepare_t(size_t smem) {
-  return cudaFuncSetAttribute(scan_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return raise_smem_limit(reinterpret_cast<const void*>(scan_kernel<G>), smem);
 }
 
 template <int G>
@@ -886,7 +912,7 @@ bool warp_vt_supported(uint32_t V) { return V == 1 || V == 2 || V == 4 || V == 8
 
 template <int G, int VT>
 static cudaError_t warp_prepare_t(size_t smem) {
-  return cudaFuncSetAttribute(scan_warp_kernel<G, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return raise_smem_limit(reinterpret_cast<const void*>(scan_warp_kernel<G, VT>), smem);
 }
 template <int G, int VT>
 static int warp_occupancy_t(size_t smem) {

@@ -9,6 +9,11 @@
 // (g_noalloc_scratch) instead of allocated buffers.  The caller passes the
 // table and the output buffer, both in device memory it already owns.
 //
+// The keys reach the array by value, inside the parameters of a small copy
+// kernel (up to kStageKeys keys per launch), so no host buffer has to outlive
+// the call and no copy from pageable memory makes the host wait for the
+// stream.
+//
 // The array is held by every GPU that loads the library until the process
 // exits.  All calls on a device share it and it keeps the last call's
 // contents: the scan kernel zeroes its own partial rows before use and the
@@ -29,15 +34,30 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // Host-side state per device: the array's device address (in host code the
-// symbol is only a stand-in and must never be passed to a kernel), the SM
-// count, and the dynamic shared memory already enabled for the scan kernel.
+// symbol is only a stand-in and must never be passed to a kernel) and the SM
+// count.  The scan kernel's shared-memory limit is not kept here: it is
+// process-wide per device and raised through mg::scan_prepare, which every
+// entry point shares.
 struct DeviceSlot {
   bool ready = false;
   unsigned char* scratch = nullptr;
   int sms = 0;
   size_t smem_optin = 0;
-  size_t prepared_smem = 0;
 };
+
+// Keys per copy launch: 16 x 624 B of kernel parameters.
+constexpr uint32_t kStageKeys = 16;
+struct KeyStage {
+  mg::KeyDev k[kStageKeys];
+  uint32_t n;
+};
+
+__global__ void stage_keys_kernel(const __grid_constant__ KeyStage s, mg::KeyDev* __restrict__ dst) {
+  const uint4* src = reinterpret_cast<const uint4*>(s.k);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  const uint32_t words = s.n * (uint32_t)(sizeof(mg::KeyDev) / 16);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) d[i] = src[i];
+}
 DeviceSlot g_slots[kMaxDevices];
 std::mutex g_mu;
 
@@ -139,11 +159,8 @@ extern "C" int mg_scan_noalloc(int device, const void* table_dev, uint64_t rows,
     const uint64_t items = tiles * nkeys;
     int occ = 0;
     if (smem <= slot->smem_optin) {
-      if (slot->prepared_smem < smem) {
-        if (mg::scan_prepare(1, smem) != cudaSuccess)
-          return noalloc_fail(MG_ECUDA, "mg_scan_noalloc: cannot set the kernel's shared memory");
-        slot->prepared_smem = smem;
-      }
+      if (mg::scan_prepare(1, smem) != cudaSuccess)
+        return noalloc_fail(MG_ECUDA, "mg_scan_noalloc: cannot set the kernel's shared memory");
       occ = mg::scan_occupancy(1, smem);
     }
     const uint64_t slots_total = (uint64_t)(occ > 0 ? occ : 1) * slot->sms;
@@ -184,10 +201,15 @@ extern "C" int mg_scan_noalloc(int device, const void* table_dev, uint64_t rows,
   p.partial = reinterpret_cast<uint4*>(slot->scratch + part_off);
 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // Pageable source: the call returns once the bytes are staged, so the
-  // stack copy may go out of scope afterwards.
-  if (cudaMemcpyAsync(slot->scratch, staged, key_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return noalloc_fail(MG_ECUDA, "mg_scan_noalloc: key upload failed");
+  // Keys travel by value in the copy kernel's parameters.
+  mg::KeyDev* const d_keys = reinterpret_cast<mg::KeyDev*>(slot->scratch);
+  for (uint32_t i0 = 0; i0 < nkeys; i0 += kStageKeys) {
+    KeyStage ks;
+    ks.n = nkeys - i0 < kStageKeys ? nkeys - i0 : kStageKeys;
+    std::memcpy(ks.k, staged + i0, ks.n * sizeof(mg::KeyDev));
+    stage_keys_kernel<<<1, 256, 0, st>>>(ks, d_keys + i0);
+    if (cudaGetLastError() != cudaSuccess) return noalloc_fail(MG_ECUDA, "mg_scan_noalloc: key upload failed");
+  }
   if (mg::launch_scan(1, p, grid, smem, st) != cudaSuccess)
     return noalloc_fail(MG_ECUDA, "mg_scan_noalloc: scan launch failed");
   if (mg::launch_reduce(p.partial, grid, p.cols, static_cast<uint4*>(out_shares_dev), st) != cudaSuccess)

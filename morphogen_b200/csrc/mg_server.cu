@@ -10,6 +10,13 @@
 // device memory (keys, frontier and partial rows of the pass), pausing drains
 // the in-flight passes so that an epoch merge can patch the tables, and the
 // loop records per-request latency for p50/p95/p99.
+//
+// Locking: one mutex guards the queues, the request table and the statistics.
+// The dispatcher holds it only to decide what to do; key parsing, planning,
+// the key upload, the launch and the read-back of a pass run with the mutex
+// released, so submit / wait / stats never wait behind a pass being planned.
+// A slot whose requests are assigned counts as in flight from the moment it
+// is claimed, so a pause waits for it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -28,6 +35,12 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Pass size when the caller sets no key cap: a pass is closed once its
+// estimated device time reaches this bound (the p99 target of a lookup), so
+// the earliest requests of a backlog are answered after one bounded pass
+// instead of after the whole backlog.
+constexpr double kPassTargetS = 0.050;
+
 struct Request {
   uint64_t id = 0;
   std::vector<const mg_table*> tables;
@@ -35,6 +48,7 @@ struct Request {
   std::vector<uint8_t> shares;
   size_t share_bytes = 0;
   uint64_t est_bytes = 0;  // device scratch estimate for admission
+  double cost = 0;         // tree nodes its keys expand (sum of the tables' rows)
   Clock::time_point t_submit, t_done;
   int status = MG_OK;
   std::string error;
@@ -71,6 +85,12 @@ struct mg_server {
   bool stop = false;
   bool paused = false;
   std::thread dispatcher;
+  uint32_t waiters = 0;   // threads inside mg_server_wait
+  bool closing = false;   // destroy is waiting for the waiters to leave
+  // Measured device rate (tree nodes per second) of completed passes, for the
+  // latency-aware pass size; 0 until the first pass completes.
+  double node_rate = 0;
+  std::vector<double> slot_cost;
   // statistics
   std::vector<double> lat_ms;
   uint64_t completed = 0, failed = 0, passes = 0, keys_done = 0;
@@ -85,16 +105,10 @@ uint32_t in_flight(const mg_server* s) {
   return n;
 }
 
-void finish_slot(mg_server* s, size_t i, int status, const char* err) {
+// Hands a slot's shares (or its error) to its requests; called with the
+// mutex held, after the shares were read back with the mutex released.
+void finish_slot(mg_server* s, size_t i, int status, const char* err, const std::vector<uint8_t>& all) {
   std::vector<Request*>& rs = s->slot_reqs[i];
-  std::vector<uint8_t> all;
-  if (status == MG_OK) {
-    size_t total = 0;
-    for (Request* r : rs) total += r->share_bytes;
-    all.resize(total);
-    status = mg_batch_read(s->slots[i], all.data(), nullptr);
-    if (status != MG_OK) err = mg_last_error();
-  }
   const auto now = Clock::now();
   size_t off = 0;
   for (Request* r : rs) {
@@ -119,11 +133,25 @@ void finish_slot(mg_server* s, size_t i, int status, const char* err) {
 void run(mg_server* s) {
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
-    // 1. Completions.
+    // 1. Completions: the slot stays claimed (in flight) while its shares
+    //    are read back with the mutex released.
     for (size_t i = 0; i < s->slots.size(); ++i) {
       if (s->slot_reqs[i].empty()) continue;
       if (!mg::batch_done(s->slots[i])) continue;
-      finish_slot(s, i, MG_OK, nullptr);
+      size_t total = 0;
+      for (Request* r : s->slot_reqs[i]) total += r->share_bytes;
+      std::vector<uint8_t> all(total);
+      lk.unlock();
+      int status = mg_batch_read(s->slots[i], all.data(), nullptr);
+      std::string err = status == MG_OK ? std::string() : std::string(mg_last_error());
+      uint64_t ns = 0;
+      if (status == MG_OK && mg_batch_last_kernel_ns(s->slots[i], &ns) != MG_OK) ns = 0;
+      lk.lock();
+      if (status == MG_OK && ns > 0 && s->slot_cost[i] > 0) {
+        const double rate = s->slot_cost[i] / ((double)ns * 1e-9);
+        s->node_rate = s->node_rate > 0 ? 0.7 * s->node_rate + 0.3 * rate : rate;
+      }
+      finish_slot(s, i, status, err.c_str(), all);
       s->cv_done.notify_all();
     }
     if (s->stop && in_flight(s) == 0) break;
@@ -132,23 +160,33 @@ void run(mg_server* s) {
       for (size_t i = 0; i < s->slots.size() && !s->pending.empty(); ++i) {
         if (!s->slot_reqs[i].empty()) continue;
         size_t free_b = 0, total_b = 0;
+        lk.unlock();  // only this thread claims slots or takes pending requests
         cudaSetDevice(mg::context_device(s->ctx));
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
           cudaGetLastError();
           free_b = 0;
         }
+        lk.lock();
+        if (s->paused || s->stop) break;
         const uint64_t budget = free_b > s->cfg.memory_reserve ? free_b - s->cfg.memory_reserve : 0;
+        // Without an explicit key cap, close the pass at the measured device
+        // time bound (always at least one request).
+        const double cost_cap = (s->cfg.max_keys_per_pass == 0 && s->node_rate > 0)
+                                    ? s->node_rate * kPassTargetS : 0.0;
         std::vector<Request*> take;
         uint64_t need = 0, nk = 0;
+        double cost = 0;
         while (!s->pending.empty()) {
           Request* r = s->pending.front();
           const bool first = take.empty();
           if (!first && s->cfg.max_keys_per_pass && nk + r->keys.size() > s->cfg.max_keys_per_pass) break;
+          if (!first && cost_cap > 0 && cost + r->cost > cost_cap) break;
           if (!first && need + r->est_bytes > budget) break;
           if (first && r->est_bytes > budget && in_flight(s) > 0) break;  // wait for memory to free up
           take.push_back(r);
           need += r->est_bytes;
           nk += r->keys.size();
+          cost += r->cost;
           s->pending.pop_front();
         }
         if (take.empty()) break;
@@ -161,9 +199,16 @@ void run(mg_server* s) {
             kp.push_back(r->keys[j].data());
             kl.push_back(r->keys[j].size());
           }
+        // Claim the slot, then plan and launch with the mutex released.  The
+        // requests' keys and tables stay valid: a request is released only by
+        // its waiter after it is done, and destroy first joins this thread.
+        s->slot_reqs[i] = take;
+        s->slot_cost[i] = cost;
+        lk.unlock();
         int rc = mg_batch_set_keys(s->slots[i], tabs.data(), kp.data(), kl.data(), (uint32_t)kp.size());
         if (rc == MG_OK) rc = mg_batch_launch(s->slots[i], nullptr);
-        s->slot_reqs[i] = take;
+        std::string err = rc == MG_OK ? std::string() : std::string(mg_last_error());
+        lk.lock();
         if (rc != MG_OK) {
           if (rc == MG_ENOMEM && in_flight(s) > 1) {
             // Memory is held by other passes: put the requests back in order.
@@ -171,7 +216,7 @@ void run(mg_server* s) {
             s->slot_reqs[i].clear();
             break;
           }
-          finish_slot(s, i, rc, mg_last_error());
+          finish_slot(s, i, rc, err.c_str(), {});
           s->cv_done.notify_all();
           continue;
         }
@@ -228,6 +273,7 @@ int mg_server_create(mg_context* ctx, const mg_server_config* cfg, mg_server** o
   }
   s->slot_reqs.resize(s->slots.size());
   s->slot_start.resize(s->slots.size());
+  s->slot_cost.assign(s->slots.size(), 0.0);
   s->t0 = Clock::now();
   s->dispatcher = std::thread(run, s);
   *out = s;
@@ -242,13 +288,28 @@ int mg_server_destroy(mg_server* s) {
     s->paused = false;
   }
   s->cv_work.notify_all();
+  // The dispatcher completes the passes already on the GPU (their requests
+  // are answered) and exits.
   if (s->dispatcher.joinable()) s->dispatcher.join();
-  for (mg_batch* b : s->slots) mg_batch_destroy(b);
-  for (Request* r : s->pending) {
-    r->status = MG_EBUSY;
-    r->done = true;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (Request* r : s->pending) {
+      r->status = MG_EBUSY;
+      r->error = "server destroyed before the request was dispatched";
+      r->t_done = Clock::now();
+      r->done = true;
+    }
+    s->pending.clear();
+    // Threads blocked in mg_server_wait wake up, take their result (MG_EBUSY
+    // for undispatched requests), release their request and leave; only
+    // then is anything freed.
+    s->closing = true;
+    s->cv_done.notify_all();
+    s->cv_done.wait(lk, [&] { return s->waiters == 0; });
+    for (auto& kv : s->reqs) delete kv.second;
+    s->reqs.clear();
   }
-  for (auto& kv : s->reqs) delete kv.second;
+  for (mg_batch* b : s->slots) mg_batch_destroy(b);
   delete s;
   return MG_OK;
 }
@@ -280,6 +341,7 @@ int mg_server_submit(mg_server* s, const mg_table* const* tables, const uint8_t*
     r->keys.emplace_back(keys[i], keys[i] + key_lens[i]);
     r->share_bytes += mg_table_row_bytes(tables[i]);
     r->est_bytes += key_scratch_bytes(tables[i], s->sms);
+    r->cost += (double)mg_table_rows(tables[i]);
   }
   r->t_submit = Clock::now();
   {
@@ -310,12 +372,18 @@ int mg_server_wait(mg_server* s, uint64_t id, uint8_t* out, uint32_t timeout_ms,
     return MG_EINVAL;
   }
   Request* r = it->second;
+  ++s->waiters;
+  auto leave = [&](int status) {
+    --s->waiters;
+    if (s->closing) s->cv_done.notify_all();
+    return status;
+  };
   auto ready = [&] { return r->done; };
   if (timeout_ms == 0) {
     s->cv_done.wait(lk, ready);
   } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
     mg::set_last_error("request not answered before the deadline");
-    return MG_ETIMEDOUT;
+    return leave(MG_ETIMEDOUT);
   }
   const int status = r->status;
   if (status == MG_OK) {
@@ -324,9 +392,9 @@ int mg_server_wait(mg_server* s, uint64_t id, uint8_t* out, uint32_t timeout_ms,
   } else {
     mg::set_last_error(r->error.c_str());
   }
-  s->reqs.erase(it);
+  s->reqs.erase(r->id);
   delete r;
-  return status;
+  return leave(status);
 }
 
 int mg_server_pause(mg_server* s, uint32_t timeout_ms) {

@@ -67,6 +67,8 @@ def lib():
         L.mgo_eval_subtree.argtypes = [kp, C.c_uint64, C.c_uint64, u32p]
         L.mgo_keygen.argtypes = [C.c_uint32, C.c_uint64, u32p, u32p, kp, kp]
         L.mgo_scan_fused.argtypes = [kp, C.c_int, u8p, C.c_uint64, C.c_uint32, C.c_uint64, u8p, C.c_int]
+        L.mgo_scan_fused_avx512.argtypes = [kp, C.c_int, u8p, C.c_uint64, C.c_uint32, C.c_uint64, u8p, C.c_int]
+        L.mgo_avx512_available.argtypes = []
         L.mgo_scan_pointwise.argtypes = [kp, u8p, C.c_uint64, C.c_uint32, u8p]
         L.mgo_delta_apply.argtypes = [kp, C.c_int, u64p, u8p, C.c_uint64, C.c_uint32, u8p]
         L.mgo_fill_splitmix.argtypes = [u8p, C.c_uint64, C.c_uint64, C.c_uint64]
@@ -155,14 +157,24 @@ def _keys_array(keys):
     return arr
 
 
-def scan_fused(keys, rows: np.ndarray, row_bytes: int, row_base: int = 0, nthreads: int = 0) -> list[bytes]:
-    """eval_fused_3dpf_cpu generalised: one share of row_bytes per key."""
+def avx512_available() -> bool:
+    return bool(lib().mgo_avx512_available())
+
+
+def scan_fused(keys, rows: np.ndarray, row_bytes: int, row_base: int = 0, nthreads: int = 0,
+               avx512: bool = False) -> list[bytes]:
+    """eval_fused_3dpf_cpu generalised: one share of row_bytes per key.
+    avx512: the AND/XOR loop in 512-bit registers, eight rows per step (the
+    shape of the reference server's AVX-512 scan); same result."""
     rows = np.ascontiguousarray(rows, dtype=np.uint8).reshape(-1)
     nrows = rows.size // row_bytes
     karr = _keys_array(keys)
     out = np.zeros(len(keys) * row_bytes, np.uint8)
-    rc = lib().mgo_scan_fused(karr, len(keys), rows.ctypes.data_as(C.POINTER(C.c_uint8)), nrows,
-                              row_bytes, row_base, out.ctypes.data_as(C.POINTER(C.c_uint8)), nthreads)
+    fn = lib().mgo_scan_fused_avx512 if avx512 else lib().mgo_scan_fused
+    rc = fn(karr, len(keys), rows.ctypes.data_as(C.POINTER(C.c_uint8)), nrows,
+            row_bytes, row_base, out.ctypes.data_as(C.POINTER(C.c_uint8)), nthreads)
+    if rc == -2:
+        raise RuntimeError("oracle: this CPU has no AVX-512F")
     if rc != 0:
         raise ValueError("oracle: scan precondition failed (more rows than domain size?)")
     return [out[i * row_bytes:(i + 1) * row_bytes].tobytes() for i in range(len(keys))]

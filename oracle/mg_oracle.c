@@ -251,9 +251,77 @@ static inline void xor_row_masked(uint32_t* acc, const uint32_t* row, const uint
 
 static uint64_t domain_size(uint32_t d) { return d >= 64 ? ~0ull : (1ull << d); }
 
-/* kernel.rs:1276-1371 */
-int mgo_scan_fused(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t nrows,
-                   uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads) {
+#if defined(__x86_64__)
+#include <immintrin.h>
+#define MGO_AVX512 __attribute__((target("avx512f")))
+
+/* The AND/XOR accumulate of rows [0, n) of one tile in 512-bit registers,
+ * eight rows per step, in the shape of the reference server's AVX-512 row
+ * scan (crates/morphogen-server/src/scan.rs:719-895, scan_chunk_avx512_inner:
+ * eight rows loaded, ANDed with their broadcast masks, XOR-folded into the
+ * accumulator).  There the mask is one DPF bit broadcast to 64 bytes; here it
+ * is the row's 16-byte DPF output repeated over its 16-byte lanes, so the
+ * result is xor_row_masked's exactly. */
+MGO_AVX512 static void xor_rows_masked_avx512(uint32_t* acc, const uint8_t* rows, const uint32_t* masks,
+                                              uint64_t n, uint32_t row_bytes) {
+  uint64_t i = 0;
+  if (row_bytes % 64 == 0) {
+    const uint32_t vecs = row_bytes / 64;
+    for (uint32_t v = 0; v < vecs; v++) {
+      __m512i a = _mm512_loadu_si512(acc + 16 * v);
+      const uint8_t* base = rows + 64 * (size_t)v;
+#define MGO_ROWV(j)                                                                          \
+  _mm512_and_si512(_mm512_loadu_si512(base + (i + (j)) * (uint64_t)row_bytes),              \
+                   _mm512_broadcast_i32x4(_mm_loadu_si128((const __m128i*)(masks + 4 * (i + (j))))))
+      for (i = 0; i + 8 <= n; i += 8) {
+        const __m512i x01 = _mm512_xor_si512(MGO_ROWV(0), MGO_ROWV(1));
+        const __m512i x23 = _mm512_xor_si512(MGO_ROWV(2), MGO_ROWV(3));
+        const __m512i x45 = _mm512_xor_si512(MGO_ROWV(4), MGO_ROWV(5));
+        const __m512i x67 = _mm512_xor_si512(MGO_ROWV(6), MGO_ROWV(7));
+        a = _mm512_xor_si512(a, _mm512_xor_si512(_mm512_xor_si512(x01, x23), _mm512_xor_si512(x45, x67)));
+      }
+      for (; i < n; i++) a = _mm512_xor_si512(a, MGO_ROWV(0));
+#undef MGO_ROWV
+      _mm512_storeu_si512(acc + 16 * v, a);
+    }
+    return;
+  }
+  if (row_bytes == 32 || row_bytes == 16) {
+    /* Several rows per vector: 32-B rows two at a time (lanes mask_i, mask_i,
+     * mask_i+1, mask_i+1), 16-B rows four at a time (the masks of rows
+     * i..i+3 are consecutive). */
+    const uint64_t per = 64 / row_bytes;
+    __m512i a = _mm512_setzero_si512();
+#define MGO_MASKV(r)                                                                          \
+  (row_bytes == 16 ? _mm512_loadu_si512(masks + 4 * (r))                                      \
+                   : _mm512_shuffle_i64x2(_mm512_castsi256_si512(_mm256_loadu_si256((const __m256i*)(masks + 4 * (r)))), \
+                                          _mm512_castsi256_si512(_mm256_loadu_si256((const __m256i*)(masks + 4 * (r)))), 0x50))
+#define MGO_VEC(r) _mm512_and_si512(_mm512_loadu_si512(rows + (r) * (uint64_t)row_bytes), MGO_MASKV(r))
+    for (i = 0; i + 8 <= n; i += 8) {
+      __m512i x = _mm512_xor_si512(MGO_VEC(i), MGO_VEC(i + per));
+      if (per == 2) x = _mm512_xor_si512(x, _mm512_xor_si512(MGO_VEC(i + 4), MGO_VEC(i + 6)));
+      a = _mm512_xor_si512(a, x);
+    }
+#undef MGO_VEC
+#undef MGO_MASKV
+    {
+      uint32_t lanes[16];
+      _mm512_storeu_si512(lanes, a);
+      for (uint32_t w = 0; w < 16; w++) acc[w % (row_bytes / 4)] ^= lanes[w];
+    }
+    for (; i < n; i++) xor_row_masked(acc, (const uint32_t*)(rows + i * (uint64_t)row_bytes), masks + 4 * i,
+                                      row_bytes / 4);
+    return;
+  }
+  for (i = 0; i < n; i++)
+    xor_row_masked(acc, (const uint32_t*)(rows + i * (uint64_t)row_bytes), masks + 4 * i, row_bytes / 4);
+}
+#endif
+
+/* kernel.rs:1276-1371.  avx512: accumulate with xor_rows_masked_avx512
+ * instead of xor_row_masked (same result). */
+static int scan_fused_impl(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t nrows,
+                           uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads, int avx512) {
   uint32_t min_d = 64, words = row_bytes / 4;
   uint64_t tile, first_tile, last_tile;
   int k;
@@ -287,6 +355,13 @@ int mgo_scan_fused(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t
       if (hi > row_base + nrows) hi = row_base + nrows;
       for (int kk = 0; kk < nkeys; kk++) {
         mgo_eval_subtree(&keys[kk], start, tile, masks);
+#if defined(__x86_64__)
+        if (avx512) {
+          xor_rows_masked_avx512(acc + (size_t)kk * words, rows + (lo - row_base) * (uint64_t)row_bytes,
+                                 masks + 4 * (lo - start), hi - lo, row_bytes);
+          continue;
+        }
+#endif
         for (i = lo; i < hi; i++)
           xor_row_masked(acc + (size_t)kk * words,
                          (const uint32_t*)(rows + (i - row_base) * (uint64_t)row_bytes),
@@ -303,6 +378,25 @@ int mgo_scan_fused(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t
     free(masks);
   }
   return 0;
+}
+
+int mgo_scan_fused(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t nrows,
+                   uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads) {
+  return scan_fused_impl(keys, nkeys, rows, nrows, row_bytes, row_base, out, nthreads, 0);
+}
+
+int mgo_avx512_available(void) {
+#if defined(__x86_64__)
+  return __builtin_cpu_supports("avx512f") ? 1 : 0;
+#else
+  return 0;
+#endif
+}
+
+int mgo_scan_fused_avx512(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t nrows,
+                          uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads) {
+  if (!mgo_avx512_available()) return -2;
+  return scan_fused_impl(keys, nkeys, rows, nrows, row_bytes, row_base, out, nthreads, 1);
 }
 
 /* kernel.rs:1374-1383 */

@@ -74,6 +74,13 @@ int mgo_scan_fused(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t
                    uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads);
 
 /* kernel.rs:1374-1383: one key, one point evaluation per row. */
+/* mgo_scan_fused with the AND/XOR loop in AVX-512 registers, eight rows per
+ * step (the shape of crates/morphogen-server/src/scan.rs:719-895); scalar
+ * ChaCha8 as the reference's CPU path.  Same result; -2 without AVX-512F. */
+int mgo_scan_fused_avx512(const mgo_key* keys, int nkeys, const uint8_t* rows, uint64_t nrows,
+                          uint32_t row_bytes, uint64_t row_base, uint8_t* out, int nthreads);
+int mgo_avx512_available(void);
+
 int mgo_scan_pointwise(const mgo_key* key, const uint8_t* rows, uint64_t nrows,
                        uint32_t row_bytes, uint8_t* out);
 

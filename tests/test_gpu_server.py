@@ -123,3 +123,80 @@ def test_deadline_and_bad_input(scanner, oracle_mod):
         srv.submit([(big, small_key)])
     srv.close()
     big.close()
+
+
+def test_destroy_wakes_a_blocked_waiter_with_ebusy(scanner, oracle_mod, tables):
+    import threading
+    srv = PirServer(scanner, slots=1)
+    srv.pause()  # the request stays pending: it is never dispatched
+    items = make_requests(oracle_mod, tables, 1, seed=3)[0]
+    rid = srv.submit(items)
+    got = {}
+
+    def waiter():
+        try:
+            srv.wait(rid)
+            got["rc"] = N.MG_OK
+        except N.MgError as e:
+            got["rc"] = e.code
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    th.join(0.2)
+    assert th.is_alive()  # blocked in mg_server_wait
+    srv.close()  # destroy: the waiter wakes with MG_EBUSY before anything is freed
+    th.join(10)
+    assert not th.is_alive() and got["rc"] == N.MG_EBUSY
+
+
+def test_submit_is_not_held_up_by_planning(scanner, oracle_mod):
+    # A 96-key pass of 31-bit keys is parsed, planned, staged and launched by
+    # the dispatcher with the server's mutex released, so submissions made
+    # meanwhile return at once.
+    import ctypes as C
+    import time
+    big = G.GpuPageMatrix.from_seed(scanner, 1 << 24, 32, seed=8)
+    srv = PirServer(scanner, slots=2)
+    keys = [oracle_keypair(oracle_mod, 31, (2654435761 * j) % (1 << 24), seed=9, i=j)[0] for j in range(96)]
+    first = srv.submit([(big, k) for k in keys])
+    small = [(big, k) for k in keys[:3]]
+    ka = N.KeyArray([bytes(k) for _, k in small])
+    tarr = (C.c_void_p * ka.n)(*[t.handle.value for t, _ in small])
+    rid = C.c_uint64()
+    ids, took = [], []
+    t_end = time.perf_counter() + 0.1
+    while time.perf_counter() < t_end:
+        t0 = time.perf_counter()
+        rc = N.lib().mg_server_submit(srv.handle, tarr, ka.ptrs, ka.lens, ka.n, C.byref(rid))
+        took.append(time.perf_counter() - t0)
+        N.check(rc)
+        srv._share_bytes[rid.value] = [32] * 3
+        ids.append(rid.value)
+        time.sleep(0.001)
+    assert max(took) < 1e-3, f"slowest submit {max(took) * 1e3:.3f} ms"
+    shares = srv.wait(first)[0]
+    assert len(shares) == 96
+    alone = scanner.scan_keys(big, keys[:3])[0]
+    for i in ids:
+        assert srv.wait(i)[0] == alone
+    srv.close()
+    big.close()
+
+
+def test_default_pass_size_follows_the_measured_rate(scanner, oracle_mod):
+    # max_keys_per_pass = 0: once a pass has been timed, a backlog whose
+    # estimated device time is above 50 ms is split into several passes.
+    t = G.GpuPageMatrix.from_seed(scanner, 1 << 24, 32, seed=10)
+    srv = PirServer(scanner, slots=1)
+    keys = [oracle_keypair(oracle_mod, 24, (40503 * j) % (1 << 24), seed=11, i=j)[0] for j in range(120)]
+    alone = srv.answer([(t, k) for k in keys[:3]])  # times one pass
+    srv.reset_stats()
+    srv.pause()
+    ids = [srv.submit([(t, k) for k in keys[3 * i:3 * i + 3]]) for i in range(40)]
+    srv.resume()
+    res = [srv.wait(i)[0] for i in ids]
+    st = srv.stats()
+    assert st["completed"] == 40 and st["passes"] >= 2
+    assert res[0] == alone
+    srv.close()
+    t.close()

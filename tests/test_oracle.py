@@ -225,3 +225,19 @@ def test_oracle_matches_reference_kernel_fixtures(oracle_mod):
             assert share[:64].hex() == case["head"][j] and share[-64:].hex() == case["tail"][j]
             if "shares" in case:
                 assert share.hex() == case["shares"][j]
+
+
+@pytest.mark.parametrize("row_bytes,nrows", [(16, 4099), (32, 5001), (64, 3000), (256, 1027), (48, 700), (4096, 40)])
+def test_avx512_scan_variant_equals_scalar(oracle_mod, row_bytes, nrows):
+    # The CPU baseline's AVX-512-shaped AND/XOR loop gives the scalar path's shares.
+    if not oracle_mod.avx512_available():
+        pytest.skip("no AVX-512F on this CPU")
+    from conftest import oracle_keypair
+    d = max(13, (nrows - 1).bit_length())
+    rows = oracle_mod.fill_splitmix(0, nrows * row_bytes, 900 + row_bytes)
+    keys = [oracle_keypair(oracle_mod, d, (97 * j) % nrows, seed=901, i=j)[0] for j in range(3)]
+    want = oracle_mod.scan_fused(keys, rows, row_bytes)
+    assert oracle_mod.scan_fused(keys, rows, row_bytes, avx512=True) == want
+    # a window that starts mid-tile
+    assert (oracle_mod.scan_fused(keys, rows[row_bytes * 37:], row_bytes, row_base=37, avx512=True)
+            == oracle_mod.scan_fused(keys, rows[row_bytes * 37:], row_bytes, row_base=37))
