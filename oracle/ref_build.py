@@ -9,12 +9,16 @@ prebuilt library is used as is.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_CUDA = Path("/root/reference/crates/morphogen-gpu-dpf/cuda")
+# The reference checkout (read-only); MORPHOGEN_REFERENCE_DIR overrides the
+# location this recipe was written against.
+REF_ROOT = Path(os.environ.get("MORPHOGEN_REFERENCE_DIR", "/root/reference"))
+REF_CUDA = REF_ROOT / "crates" / "morphogen-gpu-dpf" / "cuda"
 OUT = HERE / "_ref" / "libmg_refkernels.so"
 SOURCES = [HERE / "ref_harness.cu", REF_CUDA / "fused_kernel.cu", REF_CUDA / "fused_kernel_optimized.cu"]
 
