@@ -436,7 +436,12 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
         if combiner:
             combiner.combine(ws, stream)
         ev[i][1].record(stream)
-        scan_ns.append(ws.last_scan_ns())  # waits for this pass; device time of the scan kernel(s)
+        if not graph:
+            # Device time of the scan kernels alone (before the reduction);
+            # reading it waits for this pass.  A replayed graph is timed as a
+            # whole by the step events instead, with no host wait between
+            # passes.
+            scan_ns.append(ws.last_scan_ns())
     t_end.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -444,6 +449,8 @@ def measure(args, scanner, tables, k0, k1, targets_rows, world, local_rank, dist
         dist.barrier()
     total_ms = t_start.elapsed_time(t_end)
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    if graph:
+        scan_ns = [x * 1e6 for x in step_ms]
     if dist:
         tt = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)

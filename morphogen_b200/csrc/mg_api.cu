@@ -189,6 +189,7 @@ struct mg_batch {
     size_t smem = 0;
     int G = 1;
     uint32_t VT = 0;
+    uint32_t NW = 0;       // warp kernel: warps per CTA
     uint32_t col0 = 0;     // first share column of this launch
   };
   mg_context* ctx = nullptr;
@@ -835,14 +836,17 @@ int plan_cta(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t col0
 }
 
 // Plan one warp-kernel launch over segs (same V, at most kMaxSegs): depth-first
-// levels per lane M, chosen for load balance across the persistent warps (the
-// deepest M whose item count splits within 3% of even), or pinned as
+// levels per lane M and the CTA width (16 warps, one CTA per SM, when their
+// stacks fit the shared memory, else 8 or 4 warps).  The CTAs take their items
+// dynamically, so an SM's four schedulers finish within about one item of one
+// another; M is the deepest whose items per scheduler round up by at most 3%
+// (fewer, deeper items need fewer frontier nodes), or pinned as
 // subtree_bits = M + 5.
 int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT, uint32_t col0,
               size_t& key_cursor, std::vector<uint32_t>& key_col, std::vector<uint32_t>& key_bytes,
               std::vector<uint32_t>& key_slot, uint64_t& fr_cursor, size_t& tmp_need, mg_batch::Launch& out) {
   mg_context* ctx = b->ctx;
-  struct Cand { uint32_t M; double bal; uint64_t items; int occ; size_t smem; };
+  struct Cand { uint32_t M; double bal; uint64_t items; int occ; size_t smem; uint32_t nw; };
   std::vector<Cand> cands;
   const uint32_t pinned = b->eff_S;
   for (uint32_t Mt = 10; Mt >= 1; --Mt) {
@@ -855,23 +859,22 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
       items += (sp.keys.size() / sp.g) * ((nF + 31) / 32);
       slots = std::max(slots, M);
     }
-    const size_t smem = mg::warp_smem_bytes(G, slots);
+    uint32_t nw = (uint32_t)mg::kWarps;
+    size_t smem = mg::warp_smem_bytes(G, VT, slots, nw);
+    while (smem > ctx->smem_optin && nw > 4) {
+      nw /= 2;
+      smem = mg::warp_smem_bytes(G, VT, slots, nw);
+    }
     if (smem > ctx->smem_optin) continue;
     if (int rc = prepare_warp(ctx, G, VT, smem)) return rc;
-    const int occ = mg::warp_occupancy(G, VT, smem);
+    const int occ = mg::warp_occupancy(G, VT, smem, nw);
     if (occ <= 0) continue;
-    const uint64_t nw = (uint64_t)occ * ctx->sms * mg::kWarps;
-    // Most loaded warp under the kernel's assignment (tile-strided per
-    // segment when the key groups fit the warps, contiguous otherwise).
-    uint64_t worst = 0;
-    for (const SegPlan& sp : segs) {
-      const uint32_t M = std::min(Mt, sp.d);
-      const uint64_t tiles = (level_count(sp.table, M) + 31) / 32;
-      const uint64_t groups = sp.keys.size() / sp.g;
-      worst += (nw >= groups) ? (tiles + (nw / groups) - 1) / (nw / groups) : (groups * tiles + nw - 1) / nw;
-    }
-    const double bal = worst ? (double)items / ((double)worst * (double)nw) : 1.0;
-    cands.push_back({Mt, bal, items, occ, smem});
+    // Items per warp scheduler (4 per SM), rounded up: the last item of
+    // the busiest scheduler bounds the pass.
+    const uint64_t sched = (uint64_t)ctx->sms * 4;
+    const uint64_t worst = (items + sched - 1) / sched;
+    const double bal = worst ? (double)items / ((double)worst * (double)sched) : 1.0;
+    cands.push_back({Mt, bal, items, occ, smem, nw});
   }
   if (cands.empty()) return fail(MG_EINVAL, "no warp-kernel shape fits the device (G=%d)", G);
   const Cand* best = nullptr;
@@ -916,14 +919,16 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
       key_bytes[sp.keys[j]] = sp.table->row_bytes;
       key_slot[sp.keys[j]] = (uint32_t)(cursor + j);
     }
-    // Frontier chain: levels 0 -> F = d - M in steps of at most 8 levels.
+    // Frontier chain: levels 0 -> F = d - M in steps of at most
+    // kFrontierLevels levels (the first step takes the remainder).
     const uint32_t F = sp.d - M;
-    const uint32_t nsteps = F ? (F + 7) / 8 : 1;
+    const uint32_t FL = mg::kFrontierLevels;
+    const uint32_t nsteps = F ? (F + FL - 1) / FL : 1;
     uint32_t Lv = 0;
     for (uint32_t st = 0; st < nsteps; ++st) {
       mg::FrontierStep f;
       std::memset(&f, 0, sizeof f);
-      const uint32_t c = F ? (st == 0 ? F - 8 * (nsteps - 1) : 8u) : 0u;
+      const uint32_t c = F ? (st == 0 ? F - FL * (nsteps - 1) : FL) : 0u;
       f.L_in = Lv;
       f.c = c;
       f.n_in = Lv ? level_count(sp.table, sp.d - Lv) : 1;
@@ -950,14 +955,15 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
   L.w.cols = cols;
   L.w.slots = slots;
   L.cols = cols;
-  L.smem = mg::warp_smem_bytes(G, slots);
+  L.NW = best->nw;
+  L.smem = mg::warp_smem_bytes(G, VT, slots, L.NW);
   if (int rc = prepare_warp(ctx, G, VT, L.smem)) return rc;
-  const int occ = mg::warp_occupancy(G, VT, L.smem);
+  const int occ = mg::warp_occupancy(G, VT, L.smem, L.NW);
   if (occ <= 0) return fail(MG_EINVAL, "warp kernel does not fit the device");
   const uint64_t nctas = (uint64_t)occ * ctx->sms;
-  const uint64_t need_ctas = (items + mg::kWarps - 1) / mg::kWarps;
+  const uint64_t need_ctas = (items + L.NW - 1) / L.NW;
   L.grid = (uint32_t)std::max<uint64_t>(1, std::min(nctas, need_ctas));
-  L.nparts = L.grid * mg::kWarps;
+  L.nparts = L.grid * L.NW;
   key_cursor = cursor;
   out = std::move(L);
   return MG_OK;
@@ -974,7 +980,7 @@ static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark) {
       MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
     } else {
       for (size_t k = 0; k < L.steps.size(); ++k) MG_CUDA(mg::launch_frontier(L.steps[k], L.step_keys[k], st));
-      MG_CUDA(mg::launch_scan_warp(L.G, L.VT, L.w, L.grid, L.smem, st));
+      MG_CUDA(mg::launch_scan_warp(L.G, L.VT, L.w, L.grid, L.NW, L.smem, st));
     }
     if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
     MG_CUDA(mg::launch_reduce(b->d_partial, L.nparts, L.cols, b->d_out + L.col0, st));
@@ -992,7 +998,6 @@ namespace {
 // (b->eff_kind, b->eff_S, b->eff_G), allocate, stage the keys and copy them
 // to the device on the workspace stream.
 int plan_pass(mg_batch* b) {
-  mg_context* ctx = b->ctx;
   const uint32_t nkeys = (uint32_t)b->in_keys.size();
   std::vector<KeyDev>& parsed = b->in_keys;
   std::vector<SegPlan> segs;
@@ -1027,34 +1032,11 @@ int plan_pass(mg_batch* b) {
   const int Gc = choose_g(Vc, nc, b->eff_G, false);
   const int Gw = choose_g(Vw, nwk, b->eff_G, true);
   std::vector<SegPlan> split;
-  // Warp-kernel segments: warp w keeps key group w % groups, so when the
-  // groups do not divide the persistent warps, nw % groups warps idle.  Above
-  // 1% idle the groups are split into segments whose group counts divide the
-  // warps (largest divisor first, at most 4 segments); every segment is a
-  // separate walk over the table by all warps.  The warp count assumed is two
-  // 8-warp CTAs per SM, what the warp kernel's registers allow.
-  const uint64_t nw_est = (uint64_t)ctx->sms * 2 * mg::kWarps;
-  auto push_warp_groups = [&](const SegPlan& sp, uint32_t g, size_t full) {
-    size_t ng = full / g, at = 0;
-    for (int piece = 0; ng > 0; ++piece) {
-      size_t take = ng;
-      if (piece < 3 && (nw_est % ng) * 100 > nw_est && ng < nw_est)
-        for (size_t c = ng; c >= 1; --c)
-          if (nw_est % c == 0) { take = c; break; }
-      split.push_back(SegPlan{sp.table, sp.d,
-                              std::vector<uint32_t>(sp.keys.begin() + at, sp.keys.begin() + at + take * g), g, true});
-      at += take * g;
-      ng -= take;
-    }
-  };
   for (SegPlan& sp : segs) {
     const int G = sp.warp ? Gw : Gc;
     const uint32_t g = (uint32_t)std::min<size_t>((size_t)G, sp.keys.size());
     const size_t full = sp.keys.size() / g * g;
-    if (sp.warp && b->eff_S == 0)
-      push_warp_groups(sp, g, full);
-    else
-      split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin(), sp.keys.begin() + full), g, sp.warp});
+    split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin(), sp.keys.begin() + full), g, sp.warp});
     if (full < sp.keys.size())
       split.push_back(SegPlan{sp.table, sp.d, std::vector<uint32_t>(sp.keys.begin() + full, sp.keys.end()),
                               (uint32_t)(sp.keys.size() - full), sp.warp});
@@ -1155,7 +1137,7 @@ int plan_pass(mg_batch* b) {
     for (uint32_t si = 0; si < L.w.nsegs; ++si) {
       const mg::WarpSeg& sg = L.w.seg[si];
       const uint32_t F = sg.d - sg.M;
-      const uint32_t nsteps = F ? (F + 7) / 8 : 1;
+      const uint32_t nsteps = F ? (F + mg::kFrontierLevels - 1) / mg::kFrontierLevels : 1;
       for (uint32_t k = 0; k < nsteps; ++k, ++st) {
         mg::FrontierStep& f = L.steps[st];
         f.keys = b->d_keys + sg.key_base;
@@ -1464,6 +1446,7 @@ int mg_batch_launch_graph(mg_batch* b, void* stream) {
     add(&L.smem, sizeof L.smem);
     add(&L.G, sizeof L.G);
     add(&L.VT, sizeof L.VT);
+    add(&L.NW, sizeof L.NW);
     add(&L.col0, sizeof L.col0);
     if (L.kind == MG_KERNEL_CTA) add(&L.p, sizeof L.p);
     else add(&L.w, sizeof L.w);

@@ -220,10 +220,10 @@ struct ScanParams {
 // item is 32 consecutive frontier nodes of one key group ("warp tile", 32 x
 // 2^M rows); each lane walks its node's 2^M leaves depth-first.
 
-#ifndef MG_WARP_THREADS
-#define MG_WARP_THREADS 256
-#endif
-constexpr int kWarpThreads = MG_WARP_THREADS;  // CTA size of the warp-independent kernel
+// Widest CTA of the warp-independent kernel (16 warps, one CTA per SM: the
+// 128 registers per thread of 512 threads fill the register file); CTAs of
+// 8 or 4 warps are used when 16 warps' stacks do not fit.
+constexpr int kWarpThreads = 512;
 constexpr int kWarps = kWarpThreads / 32;
 
 struct WarpSeg {
@@ -249,16 +249,20 @@ struct WarpScanParams {
   const KeyAux* aux;    // one per key, same index as keys
   const uint4* fr_seed;
   const uint8_t* fr_t;
-  uint4* partial;       // [gridDim.x * kWarps][cols]
+  uint4* partial;       // [gridDim.x * warps per CTA][cols]
   uint64_t items;
   uint32_t nsegs;
   uint32_t cols;
   uint32_t slots;       // depth-first stack slots per key per lane (>= max M)
 };
 
+// Levels one frontier-chain step expands (its last level's 2^10 nodes fit the
+// CTA's shared memory).
+constexpr uint32_t kFrontierLevels = 10;
+
 // One breadth-first step of the frontier chain: every CTA expands one node of
-// level L_in of key blockIdx.y by c <= 8 levels and stores the first n_out
-// nodes of level L_in + c.
+// level L_in of key blockIdx.y by c <= kFrontierLevels levels and stores the
+// first n_out nodes of level L_in + c.
 struct FrontierStep {
   const KeyDev* keys;     // the segment's keys
   const uint4* in_seed;   // level L_in (unused when L_in == 0): key j at j * n_in

@@ -25,13 +25,14 @@ cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const 
 cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,
                                cudaStream_t st);
 
-// Warp-independent scan (V uint4 per row in {1,2,4,8,16,32}, G keys per warp in 1..4).
-size_t warp_smem_bytes(int G, uint32_t slots);
+// Warp-independent scan (V uint4 per row in {1,2,4,8,16,32}, G keys per warp
+// in 1..4), CTAs of nw warps (kWarps = 16 when the shared memory fits, else 8 or 4).
+size_t warp_smem_bytes(int G, uint32_t VT, uint32_t slots, uint32_t nw);
 bool warp_vt_supported(uint32_t V);
 bool warp_g_supported(int G);
 cudaError_t warp_prepare(int G, uint32_t VT, size_t smem);
-int warp_occupancy(int G, uint32_t VT, size_t smem);
-cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, size_t smem,
+int warp_occupancy(int G, uint32_t VT, size_t smem, uint32_t nw);
+cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, uint32_t nw, size_t smem,
                              cudaStream_t st);
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st);
 // Folds a table's pending delta into the shares: jobs[j] = (key slot, first share column).

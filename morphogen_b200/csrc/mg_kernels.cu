@@ -246,19 +246,30 @@ __global__ void __launch_bounds__(kThreads, (G <= 4 ? 3 : 2)) scan_kernel(const 
 // ---- warp-independent path -------------------------------------------------
 
 // Frontier chain step: CTA (node, key) expands input slot `blockIdx.x` (level
-// index in_first + slot) of level L_in of key `blockIdx.y` by c <= 8 levels
-// breadth-first in shared memory and stores the nodes of level L_in + c that
-// intersect the table, at slot (level index - out_first).
+// index in_first + slot) of level L_in of key `blockIdx.y` by c <=
+// kFrontierLevels levels breadth-first in shared memory and stores the nodes
+// of level L_in + c that intersect the table, at slot (level index -
+// out_first).  The c levels' correction words are loaded into shared memory
+// once, up front, so the level-by-level expansion (a latency chain: the top
+// levels of the tree have few nodes) waits on no memory access.
 __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constant__ FrontierStep f) {
-  __shared__ uint4 sa[kThreads], sb[kThreads];
-  __shared__ uint8_t ta[kThreads], tb[kThreads];
+  constexpr uint32_t kNodes = 1u << kFrontierLevels;
+  __shared__ uint4 sa[kNodes], sb[kNodes];
+  __shared__ uint8_t ta[kNodes], tb[kNodes];
+  __shared__ uint4 s_cw[kFrontierLevels];
+  __shared__ uint32_t s_cwl[kFrontierLevels], s_cwr[kFrontierLevels];
   const uint32_t tid = threadIdx.x;
   const uint64_t node = blockIdx.x, j = blockIdx.y;
   const uint64_t g_out0 = (f.in_first + node) << f.c;  // level index of the first child
   const uint64_t n = 1ull << f.c;
   if (g_out0 + n <= f.out_first || g_out0 >= f.out_first + f.n_out) return;  // uniform per CTA
   const KeyDev* __restrict__ K = f.keys + j;
-  if (tid == 0) {
+  if (tid < f.c) {
+    s_cw[tid] = __ldg(&K->cw_seed[f.L_in + tid]);
+    s_cwl[tid] = __ldg(&K->cw_tl[f.L_in + tid]);
+    s_cwr[tid] = __ldg(&K->cw_tr[f.L_in + tid]);
+  }
+  if (tid == 32) {
     if (f.L_in == 0) {
       sa[0] = __ldg(&K->root_seed);
       ta[0] = (uint8_t)__ldg(&K->root_t);
@@ -271,14 +282,19 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
   uint4* cs = sa; uint8_t* ct = ta;
   uint4* ns = sb; uint8_t* nt = tb;
   for (uint32_t lv = 0; lv < f.c; ++lv) {
-    if (tid < (1u << lv)) {
+    for (uint32_t i = tid; i < (1u << lv); i += kThreads) {
       uint4 Lc, Rc;
       uint32_t tl, tr;
-      expand_cw_g(cs[tid], ct[tid], K, f.L_in + lv, Lc, tl, Rc, tr);
-      ns[2 * tid] = Lc;
-      ns[2 * tid + 1] = Rc;
-      nt[2 * tid] = (uint8_t)tl;
-      nt[2 * tid + 1] = (uint8_t)tr;
+      prg_expand(cs[i], Lc, Rc, tl, tr);
+      // dpf.rs:221-239: correction word on both children when t == 1.
+      const uint32_t m = (ct[i] == 1) ? 0xFFFFFFFFu : 0u;
+      const uint4 cw = s_cw[lv];
+      Lc.x ^= cw.x & m; Lc.y ^= cw.y & m; Lc.z ^= cw.z & m; Lc.w ^= cw.w & m;
+      Rc.x ^= cw.x & m; Rc.y ^= cw.y & m; Rc.z ^= cw.z & m; Rc.w ^= cw.w & m;
+      ns[2 * i] = Lc;
+      ns[2 * i + 1] = Rc;
+      nt[2 * i] = (uint8_t)(tl ^ (s_cwl[lv] & m));
+      nt[2 * i + 1] = (uint8_t)(tr ^ (s_cwr[lv] & m));
     }
     __syncthreads();
     uint4* x = cs; cs = ns; ns = x;
@@ -300,21 +316,27 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
   atomicXor(o + 1, ((unsigned long long)v.w << 32) | v.z);
 }
 
-// Warp-independent fused expansion + scan.  Every warp keeps the same key
-// group over consecutive items (see the assignment below), so the
-// accumulators stay in registers; they are flushed (warp shuffle XOR) into
-// the warp's own partial row when the group or segment changes.  Per item each lane loads its
-// frontier node and walks its 2^M leaves depth-first (stack in the warp's
-// shared-memory slice); a step yields one leaf pair per lane for every key.
+// Warp-independent fused expansion + scan.  A CTA of W warps (16 when its
+// shared memory fits, else 8 or 4) owns a contiguous range
+// of the pass's work items, in (tile, key group) order with the groups of a
+// tile next to each other; its warps take the items one at a time from a
+// shared-memory counter, so warps that share an SMSP with fewer busy warps
+// simply take more items and every SM finishes within about one item of the
+// others.  Per item each lane loads its frontier node and walks its 2^M
+// leaves depth-first (stack in the warp's shared-memory slice); a step yields
+// one leaf pair per lane for every key.  Accumulators stay in registers and
+// are flushed (warp shuffle XOR) into the warp's own partial row when the
+// group or segment changes.
 // For rows of VT * G <= 2 uint4 each lane ANDs its own two rows with its own
 // masks.  Otherwise the masks are exchanged through shared memory with
 // __syncwarp only, and the warp scans the step's 64 rows (32 runs of 2) with
 // coalesced 128-bit loads; VT divides 32, so a lane always holds the same
-// 16-byte position of a row.  Either way the step's loads are issued before
-// the ChaCha work.
-#ifndef MG_WARP_MIN_BLOCKS
-#define MG_WARP_MIN_BLOCKS 2
-#endif
+// 16-byte position of a row.  Rows of up to 64 B are loaded before the step's
+// ChaCha work.  Wider rows (more loads per step than registers can hold) are
+// streamed: a step's rows are loaded in chunks of 8 per lane while the next
+// step's leaves are computed, one chunk consumed and the next issued after
+// every node expansion (masks double-buffered per warp), so the loads of a
+// chunk are hidden behind the expansion that follows it.
 #ifndef MG_WARP_PREFETCH
 #define MG_WARP_PREFETCH 8
 #endif
@@ -323,10 +345,11 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
 // subtree (root at tree level F, M levels deep).  The path re-joins the
 // stack (col_seed / col_t, stride 32) at relative level M - ffs(pi) (the
 // root for pi == 0), pushes the right children it passes and returns the
-// two leaf masks.
+// two leaf masks.  pump() runs after every node expansion.
+template <class Pump>
 __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const KeyAux* __restrict__ A,
                                           uint4* col_seed, int8_t* col_t, uint32_t pi, uint32_t M, uint32_t F,
-                                          uint4& ml, uint4& mr) {
+                                          uint4& ml, uint4& mr, Pump&& pump) {
   uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
   uint4 s = col_seed[lvl * 32];
   uint32_t m = (uint32_t)(int32_t)col_t[lvl * 32];
@@ -338,39 +361,49 @@ __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const Ke
     col_t[(lvl + 1) * 32] = (int8_t)mrc;
     s = Lc;
     m = mlc;
+    pump();
   }
   leaf_pair_m(s, m, A, F + M - 1, ml, mr);
+  pump();
 }
 
 template <int G, int VT>
-__global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
+__global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t slots = p.slots;
-  uint4* const base4 = reinterpret_cast<uint4*>(smem_raw);
-  uint4* const w_mask = base4 + (size_t)warp * G * 64;                                  // [G][64]
-  uint4* const w_seed = base4 + (size_t)kWarps * G * 64 + (size_t)warp * G * slots * 32;  // [G][slots][32]
-  // Stack t masks, one byte each (0 or 0xFF; sign-extended on load).
-  int8_t* const w_t = reinterpret_cast<int8_t*>(base4 + (size_t)kWarps * G * 64 + (size_t)kWarps * G * slots * 32) +
-                      (size_t)warp * G * slots * 32;
-
-  const uint64_t gw = (uint64_t)blockIdx.x * kWarps + warp;
-  const uint64_t nw = (uint64_t)gridDim.x * kWarps;
-  uint4* const my_partial = p.partial + gw * p.cols;
-  for (uint32_t c = lane; c < p.cols; c += 32) my_partial[c] = make_uint4(0u, 0u, 0u, 0u);
-  __syncwarp();
-
+  __shared__ uint32_t s_next;  // next item of this CTA's range
   constexpr int NL = 2 * VT;            // uint4 loads per lane per step
   constexpr int PF = NL < MG_WARP_PREFETCH ? NL : MG_WARP_PREFETCH;  // loads issued before the ChaCha work
   constexpr uint32_t RPL = 32 / VT;     // rows covered by one warp-wide load
-  const uint32_t pos = lane % VT, r0 = lane / VT;
-
   // Rows of at most 32 B (one key per warp) or 16 B (two): every lane scans
   // its own subtree's two rows of the step (64 contiguous bytes, whole
   // sectors) against its own leaf masks, with no shared-memory exchange and
-  // VT accumulators per key.  Wider rows use the exchange below, which keeps
-  // the loads coalesced and the register count flat.
+  // VT accumulators per key.  Wider rows use the exchange, which keeps the
+  // loads coalesced and the register count flat.
   constexpr bool OWN = VT * G <= 2;
+  constexpr bool STREAM = !OWN && NL > PF;  // rows of 128 B and more
+  constexpr int MB = STREAM ? 2 : 1;        // mask buffers per warp
+  constexpr int CH = PF;                    // loads per streamed chunk
+  constexpr uint32_t NCH = (uint32_t)(NL / CH);
+  static_assert(!STREAM || NL % CH == 0, "streamed chunks must tile the step");
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t nw = blockDim.x >> 5;
+  const uint32_t slots = p.slots;
+  uint4* const base4 = reinterpret_cast<uint4*>(smem_raw);
+  uint4* const w_mask = base4 + (size_t)warp * MB * G * 64;                                      // [MB][G][64]
+  uint4* const w_seed = base4 + (size_t)nw * MB * G * 64 + (size_t)warp * G * slots * 32;           // [G][slots][32]
+  // Stack t masks, one byte each (0 or 0xFF; sign-extended on load).
+  int8_t* const w_t = reinterpret_cast<int8_t*>(base4 + (size_t)nw * MB * G * 64 + (size_t)nw * G * slots * 32) +
+                      (size_t)warp * G * slots * 32;
+
+  const uint64_t gw = (uint64_t)blockIdx.x * nw + warp;
+  uint4* const my_partial = p.partial + gw * p.cols;
+  for (uint32_t c = lane; c < p.cols; c += 32) my_partial[c] = make_uint4(0u, 0u, 0u, 0u);
+  const uint64_t c_begin = (uint64_t)blockIdx.x * p.items / gridDim.x;
+  const uint64_t c_end = (uint64_t)(blockIdx.x + 1) * p.items / gridDim.x;
+  if (threadIdx.x == 0) s_next = 0;
+  __syncthreads();
+
+  const uint32_t pos = lane % VT, r0 = lane / VT;
   constexpr int AV = OWN ? VT : 1;
   uint4 acc[G];
   uint4 own[G][AV];
@@ -428,40 +461,66 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
     }
   };
 
-  // Work assignment, per segment.  With at most as many key groups as warps,
-  // warp gw takes group gw % groups and the tiles gw / groups + k * (W /
-  // groups), W the largest multiple of groups not above the warp count: the
-  // warp keeps one key group (accumulators stay in registers) while the
-  // groups of one tile run on neighbouring warps at the same time, so a
-  // row's later reads hit L2.  With more groups than warps, each warp takes
-  // a contiguous group-major range of items.
-  for (uint32_t si = 0; si < p.nsegs; ++si) {
-    const WarpSeg& sg = p.seg[si];
-    const uint64_t groups = sg.groups, tiles = sg.tiles;
-    const uint64_t items_s = groups * tiles;
-    const uint64_t Ws = (nw / groups) * groups;
-    uint64_t it = 0, it_end = 0, stride = 0, first_tile = 0, tile_step = 0;
-    if (Ws) {
-      if (gw >= Ws) continue;
-      first_tile = gw / groups;
-      tile_step = Ws / groups;
-      it = first_tile;
-      it_end = tiles;
-      stride = tile_step;
-    } else {
-      it = gw * items_s / nw;
-      it_end = (gw + 1) * items_s / nw;
-      stride = 1;
+  // Row stream of the wide-row path: the chunk in flight, the step it
+  // belongs to (its first load's address and the stride between loads; its
+  // masks are in buffer (gstep - 1) & 1) and the next chunk to consume (NCH:
+  // nothing in flight).  Only full warp tiles are streamed, and the stream is
+  // drained before the key group changes, so it always uses the current g.
+  uint4 cur[CH];
+  uint32_t st_j = NCH, gstep = 0, st_stride = 0, cur_g = 0;
+  const uint4* st_ptr = nullptr;
+  auto issue = [&](uint32_t j) {
+#pragma unroll
+    for (int jj = 0; jj < CH; ++jj) cur[jj] = __ldg(st_ptr + (size_t)(j * CH + (uint32_t)jj) * st_stride);
+  };
+  auto consume = [&](uint32_t j) {
+    const uint4* mk = w_mask + (size_t)((gstep - 1u) & 1u) * (G * 64);
+#pragma unroll
+    for (int jj = 0; jj < CH; ++jj) {
+      const uint32_t r = r0 + (j * CH + (uint32_t)jj) * RPL;
+#pragma unroll
+      for (int k = 0; k < G; ++k)
+        if ((uint32_t)k < cur_g) acc[k] = xor_and(acc[k], cur[jj], mk[k * 64 + r]);
     }
-    for (; it < it_end; it += stride) {
-    const uint32_t group = (uint32_t)(Ws ? gw % groups : it / tiles);
-    const uint32_t tile = (uint32_t)(Ws ? it : it % tiles);
+  };
+  auto pump = [&]() {
+    if constexpr (STREAM) {
+      if (st_j < NCH) {
+        consume(st_j);
+        if (++st_j < NCH) issue(st_j);
+      }
+    }
+  };
+  auto drain = [&]() {
+    if constexpr (STREAM) {
+      while (st_j < NCH) {
+        consume(st_j);
+        if (++st_j < NCH) issue(st_j);
+      }
+    }
+  };
+  auto no_pump = [] {};
+
+  for (;;) {
+    uint32_t rel = 0;
+    if (lane == 0) rel = atomicAdd(&s_next, 1u);
+    rel = __shfl_sync(0xFFFFFFFFu, rel, 0);
+    const uint64_t item = c_begin + rel;
+    if (item >= c_end) break;
+    uint32_t si = 0;
+    while (si + 1 < p.nsegs && item >= p.seg[si + 1].item_begin) ++si;
+    const WarpSeg& sg = p.seg[si];
+    const uint64_t local = item - sg.item_begin;
+    const uint32_t tile = (uint32_t)(local / sg.groups);
+    const uint32_t group = (uint32_t)(local % sg.groups);
     if ((int)si != cur_seg || group != cur_group) {
+      drain();
       if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
       cur_seg = (int)si;
       cur_group = group;
     }
     const uint32_t g = sg.g, M = sg.M;
+    cur_g = g;
     const uint32_t F = sg.d - M;
     const uint64_t node = (uint64_t)tile * 32 + lane;
     const bool valid = node < sg.nF;
@@ -504,7 +563,7 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
         if ((uint32_t)k >= g) break;
         uint4 ml, mr;
         leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
-                  pi, M, F, ml, mr);
+                  pi, M, F, ml, mr, no_pump);
 #pragma unroll
         for (int v = 0; v < AV; ++v) {
           own[k][v] = xor_and(own[k][v], dat[v], ml);
@@ -533,7 +592,7 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
       for (uint32_t k = 0; k < g; ++k) {
         uint4 ml, mr;
         leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
-                  pi, M, F, ml, mr);
+                  pi, M, F, ml, mr, no_pump);
         w_mask[k * 64 + 2 * lane] = ml;
         w_mask[k * 64 + 2 * lane + 1] = mr;
       }
@@ -545,15 +604,15 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
         for (int k = 0; k < G; ++k)
           if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat[jj], w_mask[k * 64 + r]);
       }
-      // Remaining loads in chunks of CH (CH divides NL - PF).
+      // Remaining loads in chunks of CH2 (CH2 divides NL - PF).
       constexpr int REST = NL - PF;
-      constexpr int CH = REST < 8 ? (REST > 0 ? REST : 1) : 8;
-      static_assert(REST % CH == 0, "load chunks must tile the step");
+      constexpr int CH2 = REST < 8 ? (REST > 0 ? REST : 1) : 8;
+      static_assert(REST % CH2 == 0, "load chunks must tile the step");
 #pragma unroll 1
-      for (int j0 = PF; j0 < NL; j0 += CH) {
-        uint4 more[CH];
+      for (int j0 = PF; j0 < NL; j0 += CH2) {
+        uint4 more[CH2];
 #pragma unroll
-        for (int jj = 0; jj < CH; ++jj) {
+        for (int jj = 0; jj < CH2; ++jj) {
           const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
           const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
           if constexpr (FULL) {
@@ -564,7 +623,7 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
           }
         }
 #pragma unroll
-        for (int jj = 0; jj < CH; ++jj) {
+        for (int jj = 0; jj < CH2; ++jj) {
           const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
 #pragma unroll
           for (int k = 0; k < G; ++k)
@@ -574,19 +633,48 @@ __global__ void __launch_bounds__(kWarpThreads, MG_WARP_MIN_BLOCKS) scan_warp_ke
       __syncwarp();
     }
     };
+    // Streamed wide rows (full tiles): the walks of step pi pump the chunks
+    // of the step before it (possibly the previous item's last step).
+    auto run_stream = [&]() {
+    for (uint32_t pi = 0; pi < pairs; ++pi) {
+      uint4* const mk = w_mask + (size_t)(gstep & 1u) * (G * 64);
+#pragma unroll 1
+      for (uint32_t k = 0; k < g; ++k) {
+        uint4 ml, mr;
+        leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
+                  pi, M, F, ml, mr, pump);
+        mk[k * 64 + 2 * lane] = ml;
+        mk[k * 64 + 2 * lane + 1] = mr;
+      }
+      drain();       // what the walks left of the previous step
+      __syncwarp();  // this step's masks visible; the other buffer free
+      ++gstep;
+      st_ptr = lp + (size_t)pi * (2 * VT);
+      st_stride = (uint32_t)jstride;
+      st_j = 0;
+      issue(0);
+    }
+    };
     if constexpr (OWN) {
       if (full)
         run_own(std::true_type{});
       else
         run_own(std::false_type{});
+    } else if constexpr (STREAM) {
+      if (full && (RPL % 2 == 0)) {
+        run_stream();
+      } else {
+        drain();
+        run_steps(std::false_type{});
+      }
     } else {
       if (full)
         run_steps(std::true_type{});
       else
         run_steps(std::false_type{});
     }
-    }
   }
+  drain();
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
 }
 
@@ -904,8 +992,11 @@ cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t 
 
 // ---- warp-path launchers --------------------------------------------------
 
-size_t warp_smem_bytes(int G, uint32_t slots) {
-  return (size_t)kWarps * G * (64 * 16 + (size_t)slots * 32 * 17);
+// Dynamic shared memory of a warp-kernel CTA of nw warps: per warp, G keys'
+// mask buffers (two for streamed wide rows) and depth-first stacks.
+size_t warp_smem_bytes(int G, uint32_t VT, uint32_t slots, uint32_t nw) {
+  const size_t mb = (2 * VT > MG_WARP_PREFETCH && VT * G > 2) ? 2 : 1;
+  return (size_t)nw * G * (mb * 64 * 16 + (size_t)slots * 32 * 17);
 }
 
 bool warp_vt_supported(uint32_t V) { return V == 1 || V == 2 || V == 4 || V == 8 || V == 16 || V == 32; }
@@ -915,15 +1006,15 @@ static cudaError_t warp_prepare_t(size_t smem) {
   return raise_smem_limit(reinterpret_cast<const void*>(scan_warp_kernel<G, VT>), smem);
 }
 template <int G, int VT>
-static int warp_occupancy_t(size_t smem) {
+static int warp_occupancy_t(size_t smem, uint32_t nw) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_warp_kernel<G, VT>, kWarpThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scan_warp_kernel<G, VT>, (int)(nw * 32), smem) != cudaSuccess)
     return 0;
   return n;
 }
 template <int G, int VT>
-static cudaError_t warp_launch_t(const WarpScanParams& p, uint32_t grid, size_t smem, cudaStream_t st) {
-  scan_warp_kernel<G, VT><<<grid, kWarpThreads, smem, st>>>(p);
+static cudaError_t warp_launch_t(const WarpScanParams& p, uint32_t grid, uint32_t nw, size_t smem, cudaStream_t st) {
+  scan_warp_kernel<G, VT><<<grid, nw * 32, smem, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -953,10 +1044,12 @@ bool warp_g_supported(int G) { return G >= 1 && G <= 4; }
 cudaError_t warp_prepare(int G, uint32_t VT, size_t smem) {
   MG_GVT_DISPATCH(G, VT, warp_prepare_t, cudaErrorInvalidValue, smem)
 }
-int warp_occupancy(int G, uint32_t VT, size_t smem) { MG_GVT_DISPATCH(G, VT, warp_occupancy_t, 0, smem) }
-cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, size_t smem,
+int warp_occupancy(int G, uint32_t VT, size_t smem, uint32_t nw) {
+  MG_GVT_DISPATCH(G, VT, warp_occupancy_t, 0, smem, nw)
+}
+cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, uint32_t nw, size_t smem,
                              cudaStream_t st) {
-  MG_GVT_DISPATCH(G, VT, warp_launch_t, cudaErrorInvalidValue, p, grid, smem, st)
+  MG_GVT_DISPATCH(G, VT, warp_launch_t, cudaErrorInvalidValue, p, grid, nw, smem, st)
 }
 
 cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, const uint64_t* idx,
