@@ -920,7 +920,9 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
       key_slot[sp.keys[j]] = (uint32_t)(cursor + j);
     }
     // Frontier chain: levels 0 -> F = d - M in steps of at most
-    // kFrontierLevels levels (the first step takes the remainder).
+    // kFrontierLevels levels.  The first step (one root per key, a latency
+    // chain) goes as deep as it can; the later, wide steps take several
+    // roots per CTA (per << c = 2^kFrontierLevels nodes).
     const uint32_t F = sp.d - M;
     const uint32_t FL = mg::kFrontierLevels;
     const uint32_t nsteps = F ? (F + FL - 1) / FL : 1;
@@ -928,9 +930,10 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
     for (uint32_t st = 0; st < nsteps; ++st) {
       mg::FrontierStep f;
       std::memset(&f, 0, sizeof f);
-      const uint32_t c = F ? (st == 0 ? F - FL * (nsteps - 1) : FL) : 0u;
+      const uint32_t c = F ? (st + 1 < nsteps ? FL : F - FL * (nsteps - 1)) : 0u;
       f.L_in = Lv;
       f.c = c;
+      f.per = st == 0 ? 1u : (1u << (FL - c));
       f.n_in = Lv ? level_count(sp.table, sp.d - Lv) : 1;
       f.in_first = Lv ? level_first(sp.table, sp.d - Lv) : 0;
       f.n_out = level_count(sp.table, sp.d - (Lv + c));

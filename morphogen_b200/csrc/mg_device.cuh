@@ -260,9 +260,9 @@ struct WarpScanParams {
 // CTA's shared memory).
 constexpr uint32_t kFrontierLevels = 10;
 
-// One breadth-first step of the frontier chain: every CTA expands one node of
-// level L_in of key blockIdx.y by c <= kFrontierLevels levels and stores the
-// first n_out nodes of level L_in + c.
+// One breadth-first step of the frontier chain: every CTA expands `per`
+// nodes of level L_in of key blockIdx.y by c <= kFrontierLevels levels and
+// stores the nodes of level L_in + c that meet the table.
 struct FrontierStep {
   const KeyDev* keys;     // the segment's keys
   const uint4* in_seed;   // level L_in (unused when L_in == 0): key j at j * n_in
@@ -277,6 +277,8 @@ struct FrontierStep {
   uint64_t out_stride;
   uint32_t L_in;
   uint32_t c;
+  uint32_t per;           // input nodes per CTA (per << c <= 2^kFrontierLevels)
+  uint32_t pad;
 };
 
 }  // namespace mg

@@ -245,13 +245,15 @@ __global__ void __launch_bounds__(kThreads, (G <= 4 ? 3 : 2)) scan_kernel(const 
 
 // ---- warp-independent path -------------------------------------------------
 
-// Frontier chain step: CTA (node, key) expands input slot `blockIdx.x` (level
-// index in_first + slot) of level L_in of key `blockIdx.y` by c <=
-// kFrontierLevels levels breadth-first in shared memory and stores the nodes
-// of level L_in + c that intersect the table, at slot (level index -
-// out_first).  The c levels' correction words are loaded into shared memory
-// once, up front, so the level-by-level expansion (a latency chain: the top
-// levels of the tree have few nodes) waits on no memory access.
+// Frontier chain step: CTA (x, key) expands the `per` consecutive input slots
+// x * per .. (level indices in_first + slot) of level L_in of key `blockIdx.y`
+// by c <= kFrontierLevels levels breadth-first in shared memory (per * 2^c <=
+// 2^kFrontierLevels nodes) and stores the nodes of level L_in + c that
+// intersect the table, at slot (level index - out_first).  Several roots per
+// CTA keep the top levels of a wide step busy; the first step (one root per
+// key) is a latency chain either way.  The c levels' correction words are
+// loaded into shared memory once, up front, so the level-by-level expansion
+// waits on no memory access.
 __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constant__ FrontierStep f) {
   constexpr uint32_t kNodes = 1u << kFrontierLevels;
   __shared__ uint4 sa[kNodes], sb[kNodes];
@@ -259,9 +261,10 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
   __shared__ uint4 s_cw[kFrontierLevels];
   __shared__ uint32_t s_cwl[kFrontierLevels], s_cwr[kFrontierLevels];
   const uint32_t tid = threadIdx.x;
-  const uint64_t node = blockIdx.x, j = blockIdx.y;
-  const uint64_t g_out0 = (f.in_first + node) << f.c;  // level index of the first child
-  const uint64_t n = 1ull << f.c;
+  const uint64_t node0 = (uint64_t)blockIdx.x * f.per, j = blockIdx.y;
+  const uint32_t nroots = (uint32_t)(f.n_in - node0 < f.per ? f.n_in - node0 : f.per);
+  const uint64_t g_out0 = (f.in_first + node0) << f.c;  // level index of the first child
+  const uint64_t n = (uint64_t)nroots << f.c;
   if (g_out0 + n <= f.out_first || g_out0 >= f.out_first + f.n_out) return;  // uniform per CTA
   const KeyDev* __restrict__ K = f.keys + j;
   if (tid < f.c) {
@@ -269,20 +272,24 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
     s_cwl[tid] = __ldg(&K->cw_tl[f.L_in + tid]);
     s_cwr[tid] = __ldg(&K->cw_tr[f.L_in + tid]);
   }
-  if (tid == 32) {
-    if (f.L_in == 0) {
+  if (f.L_in == 0) {
+    if (tid == 32) {
       sa[0] = __ldg(&K->root_seed);
       ta[0] = (uint8_t)__ldg(&K->root_t);
-    } else {
-      sa[0] = f.in_seed[j * f.n_in + node];
-      ta[0] = f.in_t[j * f.n_in + node];
+    }
+  } else {
+    for (uint32_t r = tid; r < nroots; r += kThreads) {
+      sa[r] = f.in_seed[j * f.n_in + node0 + r];
+      ta[r] = f.in_t[j * f.n_in + node0 + r];
     }
   }
   __syncthreads();
   uint4* cs = sa; uint8_t* ct = ta;
   uint4* ns = sb; uint8_t* nt = tb;
   for (uint32_t lv = 0; lv < f.c; ++lv) {
-    for (uint32_t i = tid; i < (1u << lv); i += kThreads) {
+    // Level lv holds nroots * 2^lv nodes, root-major; node i's children are
+    // 2i and 2i + 1 of the next level.
+    for (uint32_t i = tid; i < (nroots << lv); i += kThreads) {
       uint4 Lc, Rc;
       uint32_t tl, tr;
       prg_expand(cs[i], Lc, Rc, tl, tr);
@@ -331,12 +338,10 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
 // masks.  Otherwise the masks are exchanged through shared memory with
 // __syncwarp only, and the warp scans the step's 64 rows (32 runs of 2) with
 // coalesced 128-bit loads; VT divides 32, so a lane always holds the same
-// 16-byte position of a row.  Rows of up to 64 B are loaded before the step's
-// ChaCha work.  Wider rows (more loads per step than registers can hold) are
-// streamed: a step's rows are loaded in chunks of 8 per lane while the next
-// step's leaves are computed, one chunk consumed and the next issued after
-// every node expansion (masks double-buffered per warp), so the loads of a
-// chunk are hidden behind the expansion that follows it.
+// 16-byte position of a row.  The first 8 of a lane's loads of a step are
+// issued before the step's ChaCha work; wider rows load the rest after it,
+// for 128-B rows in two halves each issued before the previous batch is
+// consumed.
 #ifndef MG_WARP_PREFETCH
 #define MG_WARP_PREFETCH 8
 #endif
@@ -345,11 +350,10 @@ __device__ __forceinline__ void xor_out(uint4* out, const uint4 v) {
 // subtree (root at tree level F, M levels deep).  The path re-joins the
 // stack (col_seed / col_t, stride 32) at relative level M - ffs(pi) (the
 // root for pi == 0), pushes the right children it passes and returns the
-// two leaf masks.  pump() runs after every node expansion.
-template <class Pump>
+// two leaf masks.
 __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const KeyAux* __restrict__ A,
                                           uint4* col_seed, int8_t* col_t, uint32_t pi, uint32_t M, uint32_t F,
-                                          uint4& ml, uint4& mr, Pump&& pump) {
+                                          uint4& ml, uint4& mr) {
   uint32_t lvl = pi ? (M - (uint32_t)__ffs((int)pi)) : 0u;
   uint4 s = col_seed[lvl * 32];
   uint32_t m = (uint32_t)(int32_t)col_t[lvl * 32];
@@ -361,10 +365,8 @@ __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const Ke
     col_t[(lvl + 1) * 32] = (int8_t)mrc;
     s = Lc;
     m = mlc;
-    pump();
   }
   leaf_pair_m(s, m, A, F + M - 1, ml, mr);
-  pump();
 }
 
 template <int G, int VT>
@@ -380,19 +382,14 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
   // VT accumulators per key.  Wider rows use the exchange, which keeps the
   // loads coalesced and the register count flat.
   constexpr bool OWN = VT * G <= 2;
-  constexpr bool STREAM = !OWN && NL > PF;  // rows of 128 B and more
-  constexpr int MB = STREAM ? 2 : 1;        // mask buffers per warp
-  constexpr int CH = PF;                    // loads per streamed chunk
-  constexpr uint32_t NCH = (uint32_t)(NL / CH);
-  static_assert(!STREAM || NL % CH == 0, "streamed chunks must tile the step");
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nw = blockDim.x >> 5;
   const uint32_t slots = p.slots;
   uint4* const base4 = reinterpret_cast<uint4*>(smem_raw);
-  uint4* const w_mask = base4 + (size_t)warp * MB * G * 64;                                      // [MB][G][64]
-  uint4* const w_seed = base4 + (size_t)nw * MB * G * 64 + (size_t)warp * G * slots * 32;           // [G][slots][32]
+  uint4* const w_mask = base4 + (size_t)warp * G * 64;                                      // [G][64]
+  uint4* const w_seed = base4 + (size_t)nw * G * 64 + (size_t)warp * G * slots * 32;           // [G][slots][32]
   // Stack t masks, one byte each (0 or 0xFF; sign-extended on load).
-  int8_t* const w_t = reinterpret_cast<int8_t*>(base4 + (size_t)nw * MB * G * 64 + (size_t)nw * G * slots * 32) +
+  int8_t* const w_t = reinterpret_cast<int8_t*>(base4 + (size_t)nw * G * 64 + (size_t)nw * G * slots * 32) +
                       (size_t)warp * G * slots * 32;
 
   const uint64_t gw = (uint64_t)blockIdx.x * nw + warp;
@@ -461,45 +458,6 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
     }
   };
 
-  // Row stream of the wide-row path: the chunk in flight, the step it
-  // belongs to (its first load's address and the stride between loads; its
-  // masks are in buffer (gstep - 1) & 1) and the next chunk to consume (NCH:
-  // nothing in flight).  Only full warp tiles are streamed, and the stream is
-  // drained before the key group changes, so it always uses the current g.
-  uint4 cur[CH];
-  uint32_t st_j = NCH, gstep = 0, st_stride = 0, cur_g = 0;
-  const uint4* st_ptr = nullptr;
-  auto issue = [&](uint32_t j) {
-#pragma unroll
-    for (int jj = 0; jj < CH; ++jj) cur[jj] = __ldg(st_ptr + (size_t)(j * CH + (uint32_t)jj) * st_stride);
-  };
-  auto consume = [&](uint32_t j) {
-    const uint4* mk = w_mask + (size_t)((gstep - 1u) & 1u) * (G * 64);
-#pragma unroll
-    for (int jj = 0; jj < CH; ++jj) {
-      const uint32_t r = r0 + (j * CH + (uint32_t)jj) * RPL;
-#pragma unroll
-      for (int k = 0; k < G; ++k)
-        if ((uint32_t)k < cur_g) acc[k] = xor_and(acc[k], cur[jj], mk[k * 64 + r]);
-    }
-  };
-  auto pump = [&]() {
-    if constexpr (STREAM) {
-      if (st_j < NCH) {
-        consume(st_j);
-        if (++st_j < NCH) issue(st_j);
-      }
-    }
-  };
-  auto drain = [&]() {
-    if constexpr (STREAM) {
-      while (st_j < NCH) {
-        consume(st_j);
-        if (++st_j < NCH) issue(st_j);
-      }
-    }
-  };
-  auto no_pump = [] {};
 
   for (;;) {
     uint32_t rel = 0;
@@ -514,13 +472,11 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
     const uint32_t tile = (uint32_t)(local / sg.groups);
     const uint32_t group = (uint32_t)(local % sg.groups);
     if ((int)si != cur_seg || group != cur_group) {
-      drain();
       if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
       cur_seg = (int)si;
       cur_group = group;
     }
     const uint32_t g = sg.g, M = sg.M;
-    cur_g = g;
     const uint32_t F = sg.d - M;
     const uint64_t node = (uint64_t)tile * 32 + lane;
     const bool valid = node < sg.nF;
@@ -563,7 +519,7 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
         if ((uint32_t)k >= g) break;
         uint4 ml, mr;
         leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
-                  pi, M, F, ml, mr, no_pump);
+                  pi, M, F, ml, mr);
 #pragma unroll
         for (int v = 0; v < AV; ++v) {
           own[k][v] = xor_and(own[k][v], dat[v], ml);
@@ -592,67 +548,67 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
       for (uint32_t k = 0; k < g; ++k) {
         uint4 ml, mr;
         leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
-                  pi, M, F, ml, mr, no_pump);
+                  pi, M, F, ml, mr);
         w_mask[k * 64 + 2 * lane] = ml;
         w_mask[k * 64 + 2 * lane + 1] = mr;
       }
       __syncwarp();
+      auto load_rows = [&](uint4* buf, int j0, auto n_tag) {
+        constexpr int N = decltype(n_tag)::value;
 #pragma unroll
-      for (int jj = 0; jj < PF; ++jj) {
-        const uint32_t r = r0 + (uint32_t)jj * RPL;
-#pragma unroll
-        for (int k = 0; k < G; ++k)
-          if ((uint32_t)k < g) acc[k] = xor_and(acc[k], dat[jj], w_mask[k * 64 + r]);
-      }
-      // Remaining loads in chunks of CH2 (CH2 divides NL - PF).
-      constexpr int REST = NL - PF;
-      constexpr int CH2 = REST < 8 ? (REST > 0 ? REST : 1) : 8;
-      static_assert(REST % CH2 == 0, "load chunks must tile the step");
-#pragma unroll 1
-      for (int j0 = PF; j0 < NL; j0 += CH2) {
-        uint4 more[CH2];
-#pragma unroll
-        for (int jj = 0; jj < CH2; ++jj) {
+        for (int jj = 0; jj < N; ++jj) {
           const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
           const uint64_t row = row0 + ((uint64_t)(r >> 1) << M) + 2u * pi + (r & 1u);
           if constexpr (FULL) {
             (void)row;
-            more[jj] = __ldg(lp + (size_t)pi * (2 * VT) + (size_t)(j0 + jj) * jstride);
+            buf[jj] = __ldg(lp + (size_t)pi * (2 * VT) + (size_t)(j0 + jj) * jstride);
           } else {
-            more[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
+            buf[jj] = row < nrows ? __ldg(tbl + row * VT + pos) : make_uint4(0u, 0u, 0u, 0u);
           }
         }
+      };
+      auto use_rows = [&](const uint4* buf, int j0, auto n_tag) {
+        constexpr int N = decltype(n_tag)::value;
 #pragma unroll
-        for (int jj = 0; jj < CH2; ++jj) {
+        for (int jj = 0; jj < N; ++jj) {
           const uint32_t r = r0 + (uint32_t)(j0 + jj) * RPL;
 #pragma unroll
           for (int k = 0; k < G; ++k)
-            if ((uint32_t)k < g) acc[k] = xor_and(acc[k], more[jj], w_mask[k * 64 + r]);
+            if ((uint32_t)k < g) acc[k] = xor_and(acc[k], buf[jj], w_mask[k * 64 + r]);
+        }
+      };
+      // The rest of the step's loads (the ChaCha registers are free now).
+      // 128-B rows: two halves, each issued before the previous batch is
+      // consumed.  Wider rows: chunks of 8 (holding more of them in flight
+      // makes the kernel spill).
+      constexpr int REST = NL - PF;
+      if constexpr (REST == 0) {
+        use_rows(dat, 0, std::integral_constant<int, PF>{});
+      } else if constexpr (REST <= 8) {
+        constexpr int H = REST / 2 > 0 ? (REST % 2 == 0 ? REST / 2 : REST) : REST;
+        uint4 ma[H];
+        load_rows(ma, PF, std::integral_constant<int, H>{});
+        use_rows(dat, 0, std::integral_constant<int, PF>{});
+        if constexpr (H < REST) {
+          uint4 mb[REST - H];
+          load_rows(mb, PF + H, std::integral_constant<int, REST - H>{});
+          use_rows(ma, PF, std::integral_constant<int, H>{});
+          use_rows(mb, PF + H, std::integral_constant<int, REST - H>{});
+        } else {
+          use_rows(ma, PF, std::integral_constant<int, H>{});
+        }
+      } else {
+        use_rows(dat, 0, std::integral_constant<int, PF>{});
+        constexpr int CH2 = 8;
+        static_assert(REST % CH2 == 0, "load chunks must tile the step");
+#pragma unroll 1
+        for (int j0 = PF; j0 < NL; j0 += CH2) {
+          uint4 more[CH2];
+          load_rows(more, j0, std::integral_constant<int, CH2>{});
+          use_rows(more, j0, std::integral_constant<int, CH2>{});
         }
       }
       __syncwarp();
-    }
-    };
-    // Streamed wide rows (full tiles): the walks of step pi pump the chunks
-    // of the step before it (possibly the previous item's last step).
-    auto run_stream = [&]() {
-    for (uint32_t pi = 0; pi < pairs; ++pi) {
-      uint4* const mk = w_mask + (size_t)(gstep & 1u) * (G * 64);
-#pragma unroll 1
-      for (uint32_t k = 0; k < g; ++k) {
-        uint4 ml, mr;
-        leaf_walk(kp + k, ap + k, w_seed + (size_t)k * slots * 32 + lane, w_t + (size_t)k * slots * 32 + lane,
-                  pi, M, F, ml, mr, pump);
-        mk[k * 64 + 2 * lane] = ml;
-        mk[k * 64 + 2 * lane + 1] = mr;
-      }
-      drain();       // what the walks left of the previous step
-      __syncwarp();  // this step's masks visible; the other buffer free
-      ++gstep;
-      st_ptr = lp + (size_t)pi * (2 * VT);
-      st_stride = (uint32_t)jstride;
-      st_j = 0;
-      issue(0);
     }
     };
     if constexpr (OWN) {
@@ -660,13 +616,6 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
         run_own(std::true_type{});
       else
         run_own(std::false_type{});
-    } else if constexpr (STREAM) {
-      if (full && (RPL % 2 == 0)) {
-        run_stream();
-      } else {
-        drain();
-        run_steps(std::false_type{});
-      }
     } else {
       if (full)
         run_steps(std::true_type{});
@@ -674,7 +623,6 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
         run_steps(std::false_type{});
     }
   }
-  drain();
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
 }
 
@@ -993,10 +941,10 @@ cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t 
 // ---- warp-path launchers --------------------------------------------------
 
 // Dynamic shared memory of a warp-kernel CTA of nw warps: per warp, G keys'
-// mask buffers (two for streamed wide rows) and depth-first stacks.
+// leaf-mask exchange buffers and depth-first stacks.
 size_t warp_smem_bytes(int G, uint32_t VT, uint32_t slots, uint32_t nw) {
-  const size_t mb = (2 * VT > MG_WARP_PREFETCH && VT * G > 2) ? 2 : 1;
-  return (size_t)nw * G * (mb * 64 * 16 + (size_t)slots * 32 * 17);
+  (void)VT;
+  return (size_t)nw * G * (64 * 16 + (size_t)slots * 32 * 17);
 }
 
 bool warp_vt_supported(uint32_t V) { return V == 1 || V == 2 || V == 4 || V == 8 || V == 16 || V == 32; }
@@ -1064,7 +1012,8 @@ cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, 
 
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st) {
   if (f.n_in == 0 || nkeys == 0) return cudaSuccess;
-  dim3 grid((unsigned)f.n_in, nkeys);
+  if (f.per == 0 || ((uint64_t)f.per << f.c) > (1ull << kFrontierLevels)) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((f.n_in + f.per - 1) / f.per), nkeys);
   frontier_kernel<<<grid, kThreads, 0, st>>>(f);
   return cudaGetLastError();
 }
