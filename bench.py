@@ -650,6 +650,30 @@ def run_pages(args, scanner, hbm_peak, peaks, traffic_rec, local_rank, pages: in
     return out
 
 
+def run_pages_line(args, local_rank: int):
+    """--workload pages on one GPU: the page-mode point of the default line
+    (this library's pass against the reference's kernel on the same table and
+    keys) as its own line; --pages sets the page count (profiling cases)."""
+    import torch
+
+    from morphogen_b200 import gpu_dpf as G
+    torch.cuda.set_device(local_rank)
+    scanner = G.GpuScanner(local_rank)
+    peaks = measured_peaks()
+    try:
+        traffic_rec = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+    except (OSError, ValueError):
+        traffic_rec = {}
+    pg = run_pages(args, scanner, float(peaks["hbm_gbs"]), peaks, traffic_rec, local_rank, pages=args.pages)
+    line = {"metric": "scanned GB/s", "value": pg["GBps"], "unit": "GB/s", "n_gpus": 1,
+            "steps": pg["steps"], "warmup": pg["warmup"], "ms_per_step": pg["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": pg["workload"], "plan": pg["plan"], "cuda_graph": True,
+                       "l2": "inputs larger than L2" if args.pages * 4096 > 126e6 else "table fits L2"},
+            **{k: v for k, v in pg.items() if k not in ("workload", "plan", "steps", "warmup", "ms_per_step")}}
+    print(json.dumps(line), flush=True)
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -826,6 +850,8 @@ def main():
     ap.add_argument("--queries", default="1", help="batched31: queries per pass, or a comma list to sweep")
     ap.add_argument("--graph", action="store_true", help="replay the timed passes from a CUDA graph")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--pages", type=int, default=PAGES,
+                    help="pages workload: number of 4096-B pages (default: the reference's 16,817,159)")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain31 on one GPU: skip the c1 / batched / pages points of the default line")
     ap.add_argument("--autotune", type=int, default=-1,
@@ -854,6 +880,8 @@ def main():
             run_serve(args, local_rank)
     elif args.workload == "sharded31" and args.emulate_ranks and world == 1:
         run_emulated_shards(args, local_rank)
+    elif args.workload == "pages" and world == 1:
+        run_pages_line(args, local_rank)
     elif args.workload == "mixed":
         if rank == 0:
             run_mixed(args, local_rank)
