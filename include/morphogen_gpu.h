@@ -159,8 +159,9 @@ int mg_keygen(uint32_t domain_bits, uint64_t target, const uint8_t root_seed0[16
  * has not finished in time (the pass still completes on the device; the
  * context's internal workspace stays busy until it does).  timing may be NULL.
  * A call with the same tables, key depths and shape as the previous call on
- * the context reuses its plan and replays the pass from a CUDA graph (the
- * first such call captures it). */
+ * the context reuses its plan and replays one CUDA graph holding the key
+ * upload, the pass and the share download (the first such call captures it);
+ * its timing reports that graph's device time as kernel_ns and d2h_ns = 0. */
 int mg_scan(mg_context* ctx, const mg_table* const* tables, const uint8_t* const* keys,
             const size_t* key_lens, uint32_t nkeys, uint8_t* out_shares, uint32_t timeout_ms,
             mg_timing* timing);

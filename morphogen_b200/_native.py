@@ -200,8 +200,11 @@ class KeyArray:
     """C arrays of key pointers and lengths for one call (keeps the bytes alive)."""
 
     def __init__(self, keys: Sequence[bytes]):
-        self.keys = [bytes(k) for k in keys]
+        self.keys = [k if type(k) is bytes else bytes(k) for k in keys]
         n = len(self.keys)
-        self.ptrs = (C.POINTER(C.c_uint8) * n)(*[u8ptr(k) for k in self.keys])
+        # A char* array holds references to the bytes objects; the C side
+        # sees the same pointers as const uint8_t* const*.
+        self._arr = (C.c_char_p * n)(*self.keys)
+        self.ptrs = C.cast(self._arr, C.POINTER(C.POINTER(C.c_uint8)))
         self.lens = (C.c_size_t * n)(*[len(k) for k in self.keys])
         self.n = n

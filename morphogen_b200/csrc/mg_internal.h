@@ -17,9 +17,14 @@ bool scan_g_supported(int G);
 cudaError_t scan_prepare(int G, size_t smem);
 int scan_occupancy(int G, size_t smem);
 cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, cudaStream_t st);
+// out = XOR of the partial rows; out is cleared first unless out_zeroed.
 cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
-                          cudaStream_t st);
+                          cudaStream_t st, bool out_zeroed = false);
 cudaError_t launch_fill_splitmix(void* dst, uint64_t words, uint64_t seed, uint64_t word0, int sms, cudaStream_t st);
+// dst[i] = src[i] for n uint4 (either side may be a pinned host buffer's
+// device-mapped address) and zero[i] = 0 for nz uint4.
+cudaError_t launch_copy_u4(const void* src, void* dst, uint32_t n, cudaStream_t st, void* zero = nullptr,
+                           uint32_t nz = 0);
 cudaError_t launch_xor_rows(void* table, uint32_t V, const uint64_t* idx, const void* diffs,
                             uint64_t n, int sms, cudaStream_t st);
 cudaError_t launch_eval_points(const KeyDev* key, const uint64_t* idx, uint64_t n, void* out, int sms,

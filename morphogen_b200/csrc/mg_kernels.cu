@@ -739,6 +739,20 @@ __global__ void fill_splitmix_kernel(uint2* __restrict__ dst, uint64_t words, ui
   }
 }
 
+// dst[i] = src[i] for n 16-byte words, and zero[i] = 0 for nz.  Used
+// inside the one-call path's graph to move the keys in (clearing the shares
+// at the same time) and the shares out through the pinned host buffers'
+// device-mapped addresses: a kernel node of a few hundred threads finishes
+// sooner than a copy-engine transfer of a few KB.
+__global__ void copy_u4_kernel(const uint4* __restrict__ src, uint4* __restrict__ dst, uint32_t n,
+                               uint4* __restrict__ zero, uint32_t nz) {
+  const uint32_t m = n > nz ? n : nz;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    if (i < n) dst[i] = src[i];
+    if (i < nz) zero[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
 // table[row_idx[e]] ^= diff[e]; XOR atomics make duplicate rows in one batch
 // order-independent.
 __global__ void xor_rows_kernel(uint4* __restrict__ table, uint32_t V, const uint64_t* __restrict__ idx,
@@ -897,14 +911,24 @@ cudaError_t launch_scan(int G, const ScanParams& p, uint32_t grid, size_t smem, 
 }
 
 cudaError_t launch_reduce(const uint4* partial, uint32_t nparts, uint32_t cols, uint4* out,
-                          cudaStream_t st) {
+                          cudaStream_t st, bool out_zeroed) {
   if (cols == 0) return cudaSuccess;
-  if (cudaError_t e = cudaMemsetAsync(out, 0, (size_t)cols * 16, st)) return e;
+  if (!out_zeroed)
+    if (cudaError_t e = cudaMemsetAsync(out, 0, (size_t)cols * 16, st)) return e;
   const uint32_t cpb = cols < 32u ? cols : 32u;
   const uint32_t slices = kThreads / cpb;
   const uint32_t per_block = slices * 4;  // at most 4 partial rows per thread
   const dim3 grid((cols + cpb - 1) / cpb, nparts ? (nparts + per_block - 1) / per_block : 1);
   reduce_kernel<<<grid, kThreads, 0, st>>>(partial, nparts, cols, per_block, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_u4(const void* src, void* dst, uint32_t n, cudaStream_t st, void* zero, uint32_t nz) {
+  const uint32_t m = n > nz ? n : nz;
+  if (m == 0) return cudaSuccess;
+  const uint32_t blocks = (m + kThreads - 1) / kThreads < 32u ? (m + kThreads - 1) / kThreads : 32u;
+  copy_u4_kernel<<<blocks, kThreads, 0, st>>>(static_cast<const uint4*>(src), static_cast<uint4*>(dst), n,
+                                              static_cast<uint4*>(zero), nz);
   return cudaGetLastError();
 }
 

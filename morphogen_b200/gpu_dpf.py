@@ -420,7 +420,7 @@ class Workspace:
     def set_keys(self, tables: Sequence[GpuPageMatrix], keys: Sequence) -> None:
         if len(tables) != len(keys):
             raise ValueError("one table per key")
-        ka = N.KeyArray([bytes(k) for k in keys])
+        ka = N.KeyArray(keys)
         tarr = (C.c_void_p * ka.n)(*[t.handle.value for t in tables])
         N.check(N.lib().mg_batch_set_keys(self.handle, tarr, ka.ptrs, ka.lens, ka.n))
         self._tables, self._keys = list(tables), ka
@@ -639,7 +639,7 @@ class GpuScanner:
     def scan_keys(self, db, keys: Sequence, timeout_ms: int = 0) -> tuple[list[bytes], dict]:
         """The one-call C entry point mg_scan: host keys in, host shares out.
         `db` is one table for every key, or a sequence with one table per key."""
-        ka = N.KeyArray([bytes(k) for k in keys])
+        ka = N.KeyArray(keys)
         tabs = list(db) if isinstance(db, (list, tuple)) else [db] * ka.n
         if len(tabs) != ka.n:
             raise ValueError("one table per key")
