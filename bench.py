@@ -334,6 +334,54 @@ def run_serve(args, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
+def run_serving_point(scanner, table, rb: int, d: int, rows: int, local_rank: int) -> dict:
+    """The continuous-batching loop (mg_server) on the 2^31-row table of the
+    default line: single-lookup latency on an idle server, then one open-loop
+    Poisson point at about 60% of the one-GPU capacity for 20 s (requests of
+    1-8 lookups, mean 4; 3 keys per lookup).  One lookup's shares are checked
+    against the second server's keys (their XOR is the target row)."""
+    from morphogen_b200.server import PirServer, geometric_lookups, poisson_load
+
+    nlook = 16
+    k0, k1, targets = seeded_keys(d, rows, nlook, seed=SEED + 7)
+    lookups = [k0[3 * i:3 * i + 3] for i in range(nlook)]
+    srv = PirServer(scanner, slots=2)
+    try:
+        for _ in range(2):
+            srv.answer([(table, k) for k in lookups[1]])
+        got = srv.answer([(table, k) for k in lookups[0]])
+        other, _ = scanner.scan_keys(table, k1[0:3])
+        want = target_rows(table, targets[0:3], rb, None, local_rank)
+        verified = all(bytes(a ^ b for a, b in zip(x, y)) == w for x, y, w in zip(got, other, want))
+        srv.reset_stats()
+        for j in range(5):
+            srv.answer([(table, k) for k in lookups[j]])
+        idle = srv.stats()
+        pass_s = max(idle["p50_ms"], 1.0) * 1e-3  # one lookup = one pass when idle
+        rate = 0.6 / (4.0 * pass_s)  # requests/s at ~60% of capacity
+
+        def make_request(rng):
+            n = geometric_lookups(rng, mean=4.0, lo=1, hi=8)
+            return [(table, k) for _ in range(n) for k in lookups[int(rng.integers(0, nlook))]]
+
+        st = poisson_load(srv, make_request, rate, 20.0, seed=SEED + 8)
+    finally:
+        srv.close()
+    if not verified:
+        raise SystemExit("bench: serving-loop shares do not reconstruct the target rows")
+    return {
+        "workload": "serving loop (mg_server, 2 workspaces) over 2^31 rows x 32 B (64 GiB), 31-bit keys, "
+                    "3 keys per lookup",
+        "idle_single_lookup_ms": {"p50": round(idle["p50_ms"], 2), "p99": round(idle["p99_ms"], 2)},
+        "poisson": {"offered_req_per_s": round(st["offered_req_per_s"], 3), "requests": st["requests"],
+                    "lookups": st["keys"] // 3, "answered_lookups_per_s": round(st["answered_keys_per_s"] / 3, 3),
+                    "p50_ms": round(st["p50_ms"], 1), "p95_ms": round(st["p95_ms"], 1),
+                    "p99_ms": round(st["p99_ms"], 1), "passes": st["passes"], "failed": st["failed"],
+                    "target_load": 0.6, "duration_s": 20.0, "lookups_per_request": "geometric, mean 4, 1-8"},
+        "verified": verified,
+    }
+
+
 def expansions(first: int, n: int, d: int) -> int:
     """Tree nodes expanded by one key over rows [first, first + n): the
     internal nodes (levels of width 2^1 .. 2^d) whose leaves meet the range."""
@@ -759,6 +807,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             print(json.dumps(line), flush=True)
     if extras and rank == 0:
         line["batched"] = run_batched(args, scanner, table, prg_peak, hbm_peak, peaks, local_rank)
+        line["serving"] = run_serving_point(scanner, table, rb, d, rows, local_rank)
         table.close()
         line["c1"] = run_c1(args, scanner, prg_peak, hbm_peak, peaks, traffic_rec, local_rank)
         line["pages"] = run_pages(args, scanner, hbm_peak, peaks, traffic_rec, local_rank)
