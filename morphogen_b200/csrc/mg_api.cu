@@ -109,7 +109,7 @@ int parse_key(const uint8_t* b, size_t len, KeyDev* k) {
 }
 
 // The warp kernel's per-key constants (KeyAux): t correction bytes as
-// masks and the four possible last-level XOR terms of a leaf mask.
+// masks, and the eight last-level XOR terms of a leaf mask.
 void make_aux(const KeyDev& k, mg::KeyAux* a) {
   std::memset(a, 0, sizeof *a);
   const auto one = [](uint8_t t) { return t == 1 ? 0xFFFFFFFFu : 0u; };
@@ -117,11 +117,18 @@ void make_aux(const KeyDev& k, mg::KeyAux* a) {
   for (uint32_t l = 0; l < k.domain_bits; ++l)
     a->cw_tm[l] = make_uint4(one(k.cw_tl[l]), big(k.cw_tl[l]), one(k.cw_tr[l]), big(k.cw_tr[l]));
   const uint4 f = k.final_cw;
-  const uint4 c = k.domain_bits ? k.cw_seed[k.domain_bits - 1] : make_uint4(0u, 0u, 0u, 0u);
-  a->leaf_c[0] = make_uint4(0u, 0u, 0u, 0u);
-  a->leaf_c[1] = f;
-  a->leaf_c[2] = c;
-  a->leaf_c[3] = make_uint4(c.x ^ f.x, c.y ^ f.y, c.z ^ f.z, c.w ^ f.w);
+  const uint32_t last = k.domain_bits ? k.domain_bits - 1 : 0;
+  const uint4 c = k.domain_bits ? k.cw_seed[last] : make_uint4(0u, 0u, 0u, 0u);
+  for (uint32_t side = 0; side < 2; ++side) {
+    const uint8_t t = k.domain_bits ? (side ? k.cw_tr[last] : k.cw_tl[last]) : 0;
+    for (uint32_t p = 0; p < 2; ++p)
+      for (uint32_t b = 0; b < 2; ++b) {
+        const uint32_t child = p ? (t == 1 ? b ^ 1u : (t >= 2 ? 0u : b)) : b;
+        const uint4 cp = p ? c : make_uint4(0u, 0u, 0u, 0u);
+        const uint4 fc = child ? f : make_uint4(0u, 0u, 0u, 0u);
+        a->leaf[4 * side + 2 * p + b] = make_uint4(cp.x ^ fc.x, cp.y ^ fc.y, cp.z ^ fc.z, cp.w ^ fc.w);
+      }
+  }
 }
 
 int wait_event(cudaEvent_t ev, uint32_t timeout_ms) {

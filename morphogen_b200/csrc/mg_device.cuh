@@ -49,13 +49,16 @@ static_assert(sizeof(KeyDev) == 624, "KeyDev layout");
 // where, per level and side, one = all ones iff the t correction byte is 1
 // and big = all ones iff it is 2..255 (the child's t byte is then >= 2 and
 // never corrects).  This equals the byte rule of dpf.rs:122,192,228 exactly.
-// leaf_c[2 * p + c] = (p ? cw_seed[d - 1] : 0) ^ (c ? final_cw : 0): the
-// leaf mask of a last-level child is its PRG seed XOR leaf_c[parent t, child t].
+// A last-level child's mask is only needed to pick its leaf's XOR term, so
+// that step is a table lookup by the parent's bit p and the child's PRG bit b:
+// leaf[4 * side + 2 * p + b] = (p ? cw_seed[d - 1] : 0) ^ (c ? final_cw : 0)
+// with c the child's corrected bit (side 0 left, 1 right); the leaf mask is
+// the PRG seed XOR that entry.
 struct alignas(16) KeyAux {
   uint4 cw_tm[kMaxLevels];  // x: tl one, y: tl big, z: tr one, w: tr big (0 or ~0)
-  uint4 leaf_c[4];
+  uint4 leaf[8];
 };
-static_assert(sizeof(KeyAux) == 576, "KeyAux layout");
+static_assert(sizeof(KeyAux) == 640, "KeyAux layout");
 
 __device__ __forceinline__ uint32_t rotl16(uint32_t x) { return __byte_perm(x, 0, 0x1032); }
 __device__ __forceinline__ uint32_t rotl8(uint32_t x) { return __byte_perm(x, 0, 0x2103); }
@@ -160,16 +163,14 @@ __device__ __forceinline__ void expand_cw_m(const uint4 s, const uint32_t m, con
 
 // Last level (level d - 1): both children's leaf masks straight from the PRG
 // seeds, with the level's correction word and the final correction word
-// folded into one table lookup per child.
+// folded into one table entry per child.
 __device__ __forceinline__ void leaf_pair_m(const uint4 s, const uint32_t m, const KeyAux* __restrict__ a,
-                                            const uint32_t level, uint4& mask_l, uint4& mask_r) {
-  const uint4 tm = __ldg(&a->cw_tm[level]);
-  uint32_t tl, tr;
-  prg_expand(s, mask_l, mask_r, tl, tr);
-  const uint32_t ml = ((0u - tl) ^ (tm.x & m)) & ~(tm.y & m);
-  const uint32_t mr = ((0u - tr) ^ (tm.z & m)) & ~(tm.w & m);
-  const uint4 cl = __ldg(&a->leaf_c[(m & 2u) | (ml & 1u)]);
-  const uint4 cr = __ldg(&a->leaf_c[(m & 2u) | (mr & 1u)]);
+                                            uint4& mask_l, uint4& mask_r) {
+  uint32_t bl, br;
+  prg_expand(s, mask_l, mask_r, bl, br);
+  const uint32_t p2 = m & 2u;  // 2 * parent bit
+  const uint4 cl = __ldg(&a->leaf[p2 | bl]);
+  const uint4 cr = __ldg(&a->leaf[4u + (p2 | br)]);
   mask_l.x ^= cl.x; mask_l.y ^= cl.y; mask_l.z ^= cl.z; mask_l.w ^= cl.w;
   mask_r.x ^= cr.x; mask_r.y ^= cr.y; mask_r.z ^= cr.z; mask_r.w ^= cr.w;
 }

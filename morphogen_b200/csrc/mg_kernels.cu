@@ -366,7 +366,7 @@ __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const Ke
     s = Lc;
     m = mlc;
   }
-  leaf_pair_m(s, m, A, F + M - 1, ml, mr);
+  leaf_pair_m(s, m, A, ml, mr);
 }
 
 template <int G, int VT>
