@@ -935,21 +935,25 @@ int plan_warp(mg_batch* b, const std::vector<SegPlan>& segs, int G, uint32_t VT,
       key_bytes[sp.keys[j]] = sp.table->row_bytes;
       key_slot[sp.keys[j]] = (uint32_t)(cursor + j);
     }
-    // Frontier chain: levels 0 -> F = d - M in steps of at most
-    // kFrontierLevels levels.  The first step (one root per key, a latency
-    // chain) goes as deep as it can; the later, wide steps take several
-    // roots per CTA (per << c = 2^kFrontierLevels nodes).
+    // Frontier chain: levels 0 -> F = d - M.  Up to kFrontierLevels levels
+    // it is one step from each key's root.  Deeper, every step expands
+    // kFrontierLevels levels below one root per CTA, and the first step's
+    // CTAs reach their roots (level A = F - kFrontierLevels * nsteps, 1..10)
+    // by walking the path from the key's root themselves, so no narrow
+    // one-CTA-per-key step sits above them.
     const uint32_t F = sp.d - M;
     const uint32_t FL = mg::kFrontierLevels;
-    const uint32_t nsteps = F ? (F + FL - 1) / FL : 1;
-    uint32_t Lv = 0;
+    const uint32_t nsteps = F <= FL ? 1u : (F - 1) / FL;
+    const uint32_t A = F <= FL ? 0u : F - FL * nsteps;
+    uint32_t Lv = A;
     for (uint32_t st = 0; st < nsteps; ++st) {
       mg::FrontierStep f;
       std::memset(&f, 0, sizeof f);
-      const uint32_t c = F ? (st + 1 < nsteps ? FL : F - FL * (nsteps - 1)) : 0u;
+      const uint32_t c = F <= FL ? F : FL;
       f.L_in = Lv;
       f.c = c;
-      f.per = st == 0 ? 1u : (1u << (FL - c));
+      f.per = 1u;
+      f.walk = (st == 0 && A > 0) ? 1u : 0u;
       f.n_in = Lv ? level_count(sp.table, sp.d - Lv) : 1;
       f.in_first = Lv ? level_first(sp.table, sp.d - Lv) : 0;
       f.n_out = level_count(sp.table, sp.d - (Lv + c));
@@ -997,12 +1001,28 @@ static int enqueue_pass(mg_batch* b, cudaStream_t st, cudaEvent_t mark, bool out
     const mg_batch::Launch& L = b->launches[i];
     if (L.kind == MG_KERNEL_CTA) {
       MG_CUDA(mg::launch_scan(L.G, L.p, L.grid, L.smem, st));
-    } else {
+    } else if (!mg::warp_reduces_in_kernel(L.G, L.VT)) {
       for (size_t k = 0; k < L.steps.size(); ++k) MG_CUDA(mg::launch_frontier(L.steps[k], L.step_keys[k], st));
+      MG_CUDA(mg::launch_scan_warp(L.G, L.VT, L.w, L.grid, L.NW, L.smem, st));
+    } else {
+      // The scan CTAs reduce into the shares themselves; the first frontier
+      // step zeroes them (a memset when no frontier step runs).
+      bool zeroed = out_zeroed || L.cols == 0;
+      for (size_t k = 0; k < L.steps.size(); ++k) {
+        mg::FrontierStep f = L.steps[k];
+        if (!zeroed && f.n_in > 0 && L.step_keys[k] > 0) {
+          f.zero_out = b->d_out + L.col0;
+          f.zero_n = L.cols;
+          zeroed = true;
+        }
+        MG_CUDA(mg::launch_frontier(f, L.step_keys[k], st));
+      }
+      if (!zeroed) MG_CUDA(cudaMemsetAsync(b->d_out + L.col0, 0, (size_t)L.cols * 16, st));
       MG_CUDA(mg::launch_scan_warp(L.G, L.VT, L.w, L.grid, L.NW, L.smem, st));
     }
     if (mark && i + 1 == b->launches.size()) MG_CUDA(cudaEventRecord(mark, st));
-    MG_CUDA(mg::launch_reduce(b->d_partial, L.nparts, L.cols, b->d_out + L.col0, st, out_zeroed));
+    if (L.kind == MG_KERNEL_CTA || !mg::warp_reduces_in_kernel(L.G, L.VT))
+      MG_CUDA(mg::launch_reduce(b->d_partial, L.nparts, L.cols, b->d_out + L.col0, st, out_zeroed));
   }
   for (const mg_batch::DeltaLaunch& dl : b->deltas)
     MG_CUDA(mg::launch_delta(b->d_keys, b->d_jobs + dl.job0, dl.njobs, dl.table->d_delta_idx, dl.table->d_delta_diff,
@@ -1151,12 +1171,13 @@ int plan_pass(mg_batch* b) {
     L.w.fr_seed = b->d_fr_seed;
     L.w.fr_t = b->d_fr_t;
     L.w.partial = b->d_partial;
+    L.w.out = b->d_out + L.col0;
     // Wire the frontier chains: each segment's steps are consecutive.
     size_t st = 0;
     for (uint32_t si = 0; si < L.w.nsegs; ++si) {
       const mg::WarpSeg& sg = L.w.seg[si];
       const uint32_t F = sg.d - sg.M;
-      const uint32_t nsteps = F ? (F + mg::kFrontierLevels - 1) / mg::kFrontierLevels : 1;
+      const uint32_t nsteps = F <= mg::kFrontierLevels ? 1u : (F - 1) / mg::kFrontierLevels;
       for (uint32_t k = 0; k < nsteps; ++k, ++st) {
         mg::FrontierStep& f = L.steps[st];
         f.keys = b->d_keys + sg.key_base;
@@ -1205,7 +1226,9 @@ int plan_pass(mg_batch* b) {
   }
   b->info.frontier_nodes = (uint32_t)std::min<uint64_t>(fr_cursor, 0xFFFFFFFFu);
   b->info.kernels = 0;
-  for (const mg_batch::Launch& L : b->launches) b->info.kernels += 2 + (uint32_t)L.steps.size();
+  for (const mg_batch::Launch& L : b->launches)
+    b->info.kernels += (L.kind == MG_KERNEL_CTA || !mg::warp_reduces_in_kernel(L.G, L.VT) ? 2u : 1u) +
+                       (uint32_t)L.steps.size();
   b->info.kernels += (uint32_t)b->deltas.size();
   b->planned = true;
   return MG_OK;

@@ -251,6 +251,7 @@ struct WarpScanParams {
   const uint4* fr_seed;
   const uint8_t* fr_t;
   uint4* partial;       // [gridDim.x * warps per CTA][cols]
+  uint4* out;           // the launch's cols shares (wide rows: zeroed before the launch, CTAs XOR into them)
   uint64_t items;
   uint32_t nsegs;
   uint32_t cols;
@@ -263,7 +264,10 @@ constexpr uint32_t kFrontierLevels = 10;
 
 // One breadth-first step of the frontier chain: every CTA expands `per`
 // nodes of level L_in of key blockIdx.y by c <= kFrontierLevels levels and
-// stores the nodes of level L_in + c that meet the table.
+// stores the nodes of level L_in + c that meet the table.  With `walk` set
+// (per == 1) the CTA's root is not read from in_seed: the CTA derives it from
+// the key's root by the L_in-level path walk of ChaCha::eval, so the first
+// step of a chain needs no narrow one-CTA-per-key launch above it.
 struct FrontierStep {
   const KeyDev* keys;     // the segment's keys
   const uint4* in_seed;   // level L_in (unused when L_in == 0): key j at j * n_in
@@ -279,7 +283,9 @@ struct FrontierStep {
   uint32_t L_in;
   uint32_t c;
   uint32_t per;           // input nodes per CTA (per << c <= 2^kFrontierLevels)
-  uint32_t pad;
+  uint32_t walk;          // 1: each CTA walks from the key's root to its level-L_in node
+  uint4* zero_out;        // CTA (0, 0) zeroes these zero_n shares first (or null)
+  uint64_t zero_n;
 };
 
 }  // namespace mg

@@ -37,6 +37,7 @@ bool warp_vt_supported(uint32_t V);
 bool warp_g_supported(int G);
 cudaError_t warp_prepare(int G, uint32_t VT, size_t smem);
 int warp_occupancy(int G, uint32_t VT, size_t smem, uint32_t nw);
+bool warp_reduces_in_kernel(int G, uint32_t VT);
 cudaError_t launch_scan_warp(int G, uint32_t VT, const WarpScanParams& p, uint32_t grid, uint32_t nw, size_t smem,
                              cudaStream_t st);
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st);

@@ -262,6 +262,9 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
   __shared__ uint32_t s_cwl[kFrontierLevels], s_cwr[kFrontierLevels];
   const uint32_t tid = threadIdx.x;
   const uint64_t node0 = (uint64_t)blockIdx.x * f.per, j = blockIdx.y;
+  // The pass's shares start at zero: the scan CTAs XOR into them.
+  if (f.zero_out && blockIdx.x == 0 && blockIdx.y == 0)
+    for (uint64_t i = tid; i < f.zero_n; i += kThreads) f.zero_out[i] = make_uint4(0u, 0u, 0u, 0u);
   const uint32_t nroots = (uint32_t)(f.n_in - node0 < f.per ? f.n_in - node0 : f.per);
   const uint64_t g_out0 = (f.in_first + node0) << f.c;  // level index of the first child
   const uint64_t n = (uint64_t)nroots << f.c;
@@ -272,10 +275,26 @@ __global__ void __launch_bounds__(kThreads) frontier_kernel(const __grid_constan
     s_cwl[tid] = __ldg(&K->cw_tl[f.L_in + tid]);
     s_cwr[tid] = __ldg(&K->cw_tr[f.L_in + tid]);
   }
-  if (f.L_in == 0) {
-    if (tid == 32) {
-      sa[0] = __ldg(&K->root_seed);
-      ta[0] = (uint8_t)__ldg(&K->root_t);
+  if (f.L_in == 0 || f.walk) {
+    // The CTA's root (per == 1 when walking): node in_first + node0 of level
+    // L_in, reached from the key's root as ChaCha::eval does (dpf.rs:103-142).
+    // Warp 1 walks while warp 0 loads the step's correction words.
+    if ((tid >> 5) == 1) {
+      uint4 s = __ldg(&K->root_seed);
+      uint32_t t = __ldg(&K->root_t);
+      const uint64_t a = f.in_first + node0;
+      for (uint32_t lvl = 0; lvl < f.L_in; ++lvl) {
+        uint4 Lc, Rc;
+        uint32_t tl, tr;
+        expand_cw_g(s, t, K, lvl, Lc, tl, Rc, tr);
+        const uint32_t bit = (uint32_t)(a >> (f.L_in - 1 - lvl)) & 1u;
+        s = bit ? Rc : Lc;
+        t = bit ? tr : tl;
+      }
+      if (tid == 32) {
+        sa[0] = s;
+        ta[0] = (uint8_t)t;
+      }
     }
   } else {
     for (uint32_t r = tid; r < nroots; r += kThreads) {
@@ -624,7 +643,28 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
     }
   }
   if (cur_seg >= 0) flush(p.seg[cur_seg], cur_group);
+  if constexpr (!OWN) {
+    // Cross-block reduction of the wide-row instantiations: the CTA XORs its
+    // warps' partial rows (written by this CTA, visible after the barrier;
+    // plain loads, not the read-only path) and folds the result into the
+    // zeroed shares with 64-bit XOR atomics.  XOR is associative and
+    // commutative, so the shares do not depend on the order.  (The own-rows
+    // instantiations leave this to reduce_kernel: the extra code changes
+    // their register allocation and costs 0.5% on the 31-bit pass, far more
+    // than the reduction launch it saves.)
+    __syncthreads();
+    const uint4* const cta_part = p.partial + (uint64_t)blockIdx.x * nw * p.cols;
+    for (uint32_t c = threadIdx.x; c < p.cols; c += blockDim.x) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      for (uint32_t w = 0; w < nw; ++w) v = xor4(v, cta_part[(size_t)w * p.cols + c]);
+      xor_out(p.out + c, v);
+    }
+  }
 }
+
+// Whether scan_warp_kernel<G, VT> reduces its partial rows into the shares
+// itself (wide rows) or leaves them to reduce_kernel (own-rows scan).
+bool warp_reduces_in_kernel(int G, uint32_t VT) { return (uint32_t)G * VT > 2u; }
 
 // out[c] ^= XOR over the nparts partial rows (launch_reduce zeroes out first).
 // Block (x, y) = cpb columns x (kThreads / cpb) slices over the partial rows
@@ -1037,6 +1077,7 @@ cudaError_t launch_delta(const KeyDev* keys, const uint2* jobs, uint32_t njobs, 
 cudaError_t launch_frontier(const FrontierStep& f, uint32_t nkeys, cudaStream_t st) {
   if (f.n_in == 0 || nkeys == 0) return cudaSuccess;
   if (f.per == 0 || ((uint64_t)f.per << f.c) > (1ull << kFrontierLevels)) return cudaErrorInvalidValue;
+  if (f.walk && (f.per != 1 || f.L_in >= (uint32_t)kMaxLevels)) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((f.n_in + f.per - 1) / f.per), nkeys);
   frontier_kernel<<<grid, kThreads, 0, st>>>(f);
   return cudaGetLastError();
