@@ -388,6 +388,29 @@ __device__ __forceinline__ void leaf_walk(const KeyDev* __restrict__ K, const Ke
   leaf_pair_m(s, m, A, ml, mr);
 }
 
+// Two depth-first steps at once (M >= 2): node q of relative level M - 2,
+// whose children are the nodes of leaf pairs 2q and 2q + 1.  The path
+// re-joins the stack at relative level M - 1 - ffs(q) (the root for q == 0),
+// pushes the right children it passes and expands node q itself, so the
+// second child stays in registers instead of taking a stack round trip.
+__device__ __forceinline__ void pair_walk(const KeyDev* __restrict__ K, const KeyAux* __restrict__ A,
+                                          uint4* col_seed, int8_t* col_t, uint32_t q, uint32_t M, uint32_t F,
+                                          uint4& s0, uint32_t& m0, uint4& s1, uint32_t& m1) {
+  uint32_t lvl = q ? (M - 1 - (uint32_t)__ffs((int)q)) : 0u;
+  uint4 s = col_seed[lvl * 32];
+  uint32_t m = (uint32_t)(int32_t)col_t[lvl * 32];
+  for (; lvl < M - 2; ++lvl) {
+    uint4 Lc, Rc;
+    uint32_t mlc, mrc;
+    expand_cw_m(s, m, K, A, F + lvl, Lc, mlc, Rc, mrc);
+    col_seed[(lvl + 1) * 32] = Rc;
+    col_t[(lvl + 1) * 32] = (int8_t)mrc;
+    s = Lc;
+    m = mlc;
+  }
+  expand_cw_m(s, m, K, A, F + M - 2, s0, m0, s1, m1);
+}
+
 template <int G, int VT>
 __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid_constant__ WarpScanParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -522,6 +545,38 @@ __global__ void __launch_bounds__(kWarpThreads, 1) scan_warp_kernel(const __grid
     const uint4* const own_lp = full ? tbl + (row0 + ((uint64_t)lane << M)) * VT : tbl;
     auto run_own = [&](auto full_tag) {
     constexpr bool FULL = decltype(full_tag)::value;
+    if constexpr (FULL && G == 1) {
+      // Odd leaf pairs are the right children of the even steps' last
+      // expansion: they stay in registers (carry) instead of taking a
+      // stack round trip.
+      if (M >= 2) {
+        const KeyDev* __restrict__ K0 = kp;
+        const KeyAux* __restrict__ A0 = ap;
+        uint4 carry_s = make_uint4(0u, 0u, 0u, 0u);
+        uint32_t carry_m = 0u;
+        for (uint32_t pi = 0; pi < pairs; ++pi) {
+          uint4 dat[2 * AV];
+#pragma unroll
+          for (int j = 0; j < 2 * AV; ++j) dat[j] = __ldg(own_lp + (size_t)pi * (2 * VT) + j);
+          uint4 sl;
+          uint32_t msl;
+          if (pi & 1u) {
+            sl = carry_s;
+            msl = carry_m;
+          } else {
+            pair_walk(K0, A0, w_seed + lane, w_t + lane, pi >> 1, M, F, sl, msl, carry_s, carry_m);
+          }
+          uint4 ml, mr;
+          leaf_pair_m(sl, msl, A0, ml, mr);
+#pragma unroll
+          for (int v = 0; v < AV; ++v) {
+            own[0][v] = xor_and(own[0][v], dat[v], ml);
+            own[0][v] = xor_and(own[0][v], dat[AV + v], mr);
+          }
+        }
+        return;
+      }
+    }
     for (uint32_t pi = 0; pi < pairs; ++pi) {
       uint4 dat[2 * AV];
 #pragma unroll
