@@ -551,10 +551,12 @@ def rooflines(bytes_scanned: int, nodes: int, seconds: float, prg_peak: float, h
     return {"bound": "hbm", **hbm, "traffic": traffic, "alu": alu}
 
 
-def traffic_for(traffic_rec: dict, kernel_kind: int, bytes_scanned: int):
+def traffic_for(traffic_rec: dict, kernel_kind: int, bytes_scanned: int, row_bytes: int = 32):
     """DRAM read + write bytes per launch: the ratio ncu measured on a smaller
-    capture of the same kernel, scaled by the rows scanned."""
-    rec = traffic_rec.get("scan_warp_kernel" if kernel_kind == 2 else "scan_kernel", {})
+    capture of the same kernel (the warp kernel's own-rows and wide-row
+    instantiations apart), scaled by the rows scanned."""
+    name = "scan_kernel" if kernel_kind != 2 else ("scan_warp_kernel" if row_bytes <= 32 else "scan_warp_kernel_wide")
+    rec = traffic_rec.get(name, {})
     if not rec.get("table_bytes"):
         return None
     return round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_scanned)
@@ -581,8 +583,8 @@ def run_c1(args, scanner, prg_peak, hbm_peak, peaks, traffic_rec, local_rank) ->
         "e2e": {"value": round(bytes_pass / (m["e2e_per"] * 1e-3) / 1e9, 2), "unit": "GB/s",
                 "ms": round(m["e2e_per"], 4), **{f"{k}_ms": v for k, v in pct3(m["e2e_ms"]).items()}},
         "roofline": rooflines(bytes_pass, nodes, m["scan_avg_s"], prg_peak, hbm_peak, peaks,
-                              traffic_for(traffic_rec, m["plan"].get("kernel"), bytes_pass)),
-        "roofline_note": "a replayed pass is timed as a whole (frontier chain, scan and reduction kernels)",
+                              traffic_for(traffic_rec, m["plan"].get("kernel"), bytes_pass, rb)),
+        "roofline_note": "a replayed pass is timed as a whole (frontier and scan kernels; the scan reduces in-kernel)",
         "verified": m["verified"], "clocks": m["clocks"], "l2": "table (268 MB) larger than L2 (126 MB)",
     }
     if not args.no_cpu:
@@ -773,7 +775,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         local_bytes = n_local * rb
         nodes = nkeys * expansions(first, n_local, d)
         roof = rooflines(local_bytes, nodes, m["scan_avg_s"], prg_peak, hbm_peak, peaks,
-                         traffic_for(traffic_rec, plan.get("kernel"), local_bytes) if nkeys == 3 else None)
+                         traffic_for(traffic_rec, plan.get("kernel"), local_bytes, rb) if nkeys == 3 else None)
         roof["timed"] = "frontier chain + scan kernel of each pass (CUDA events before the reduction)"
         if rank != 0:
             continue
