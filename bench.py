@@ -354,7 +354,7 @@ def run_serving_point(scanner, table, rb: int, d: int, rows: int, local_rank: in
         want = target_rows(table, targets[0:3], rb, None, local_rank)
         verified = all(bytes(a ^ b for a, b in zip(x, y)) == w for x, y, w in zip(got, other, want))
         srv.reset_stats()
-        for j in range(5):
+        for j in range(9):
             srv.answer([(table, k) for k in lookups[j]])
         idle = srv.stats()
         pass_s = max(idle["p50_ms"], 1.0) * 1e-3  # one lookup = one pass when idle
