@@ -130,6 +130,37 @@ def test_every_warp_kernel_shape_is_bit_exact(scanner, oracle_mod, warp_tile_bit
     ws.close()
 
 
+@pytest.mark.parametrize("rb", [32, 64])
+@pytest.mark.parametrize("d,M", [(16, 5), (20, 10), (21, 10), (22, 1), (30, 10), (31, 10), (32, 2), (32, 1)])
+def test_frontier_chain_depths_are_bit_exact(scanner, oracle_mod, d, M, rb):
+    # F = d - M frontier levels: one step from the roots up to 10 levels,
+    # else steps of 10 levels whose first reaches its roots by a path walk
+    # of F - 10 * steps levels (1..10).  The table is a row range that does
+    # not start on a tile boundary, so every step keeps only the nodes that
+    # meet the rows.  32-B rows use reduce_kernel, 64-B rows reduce in-kernel
+    # with the shares zeroed by the first frontier step.
+    n = 40_000
+    first = ((1 << d) - n) // 3 + 3
+    db = G.GpuPageMatrix.from_seed(scanner, n, rb, seed=81, first_row=first)
+    host = oracle_mod.fill_splitmix(first * rb, n * rb, 81).reshape(n, rb)
+    keys = [oracle_keypair(oracle_mod, d, first + (12_347 * j) % n, seed=82, i=j)[0] for j in range(3)]
+    ws = scanner.workspace()
+    ws.set_kernel("warp")
+    ws.set_shape(M + 5, 1)
+    ws.set_keys([db] * 3, keys)
+    ws.launch()
+    assert ws.read() == oracle_mod.scan_fused(keys, host, rb, row_base=first)
+    F = d - M
+    steps = 1 if F <= 10 else (F - 1) // 10
+    plan = ws.plan()
+    assert plan["subtree_bits"] == M + 5
+    assert plan["kernels"] == steps + (1 if rb > 32 else 2)
+    ws.launch(graph=True)
+    assert ws.read() == oracle_mod.scan_fused(keys, host, rb, row_base=first)
+    ws.close()
+    db.close()
+
+
 def test_domain_zero_key(scanner, oracle_mod):
     # from_bytes accepts d = 0 (a one-leaf domain, dpf.rs:277-316).
     k0, _ = oracle_keypair(oracle_mod, 4, 3)
