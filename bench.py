@@ -559,7 +559,9 @@ def traffic_for(traffic_rec: dict, kernel_kind: int, bytes_scanned: int, row_byt
     rec = traffic_rec.get(name, {})
     if not rec.get("table_bytes"):
         return None
-    return round((rec["dram_read_bytes"] + rec["dram_write_bytes"]) / rec["table_bytes"] * bytes_scanned)
+    # Reads grow with the rows scanned; the writes are the per-CTA partial
+    # rows and shares, which do not, so they are added as captured.
+    return round(rec["dram_read_bytes"] / rec["table_bytes"] * bytes_scanned + rec["dram_write_bytes"])
 
 
 def run_c1(args, scanner, prg_peak, hbm_peak, peaks, traffic_rec, local_rank) -> dict:
