@@ -6,7 +6,9 @@ size-independent properties (tolerance: bit-exact):
   * a pending delta changes each share by exactly the oracle's delta term
     (linearity of the scan, scan.rs:434-485);
   * the keys' shares over a 2^20-row window deep in the domain equal the
-    oracle's scan of the same window at the same logical rows."""
+    oracle's scan of the same window at the same logical rows;
+  * with a 2^28 x 64 B accounts table resident beside it, one pass over both
+    tables reconstructs every target row of both."""
 import numpy as np
 import pytest
 
@@ -63,3 +65,38 @@ def test_deep_window_matches_oracle(scanner, oracle_mod):
     host = oracle_mod.fill_splitmix(first * RB, n * RB, 0)
     assert got == oracle_mod.scan_fused(keys, host, RB, row_base=first)
     win.close()
+
+
+def test_full_size_mixed_tables_one_pass_reconstruct(scanner, oracle_mod, big):
+    """Two resident tables in one pass at full size: an accounts table of
+    2^28 rows x 64 B (16 GiB, 28-bit keys) beside the 2^31 x 32 B storage
+    table (31-bit keys).  Both servers' passes hold 2 accounts queries and 1
+    storage query; every share pair XORs to its target row."""
+    arows, arb, ad = 1 << 28, 64, 28
+    free = scanner.device_info()["free_bytes"]
+    if free < arows * arb + (4 << 30):
+        pytest.skip(f"needs {arows * arb >> 30} GiB more free device memory")
+    acc = G.GpuPageMatrix.from_seed(scanner, arows, arb, seed=1)
+    try:
+        at = [int(x) for x in np.random.default_rng(5).integers(0, arows, 6)]
+        at[0] = arows - 1
+        st = [int(x) for x in np.random.default_rng(6).integers(0, ROWS, 3)]
+        pairs = [oracle_keypair(oracle_mod, ad, t, seed=35, i=j) for j, t in enumerate(at)]
+        pairs += [oracle_keypair(oracle_mod, D, t, seed=36, i=j) for j, t in enumerate(st)]
+        tables = [acc] * 6 + [big] * 3
+        shares = []
+        for side in (0, 1):
+            ws = scanner.workspace()
+            ws.set_keys(tables, [p[side] for p in pairs])
+            ws.launch()
+            shares.append(ws.read())
+            assert ws.plan()["segments"] == 2
+            ws.close()
+        for j, t in enumerate(at):
+            want = oracle_mod.fill_splitmix(t * arb, arb, 1).tobytes()
+            assert xor_bytes(shares[0][j], shares[1][j]) == want
+        for j, t in enumerate(st):
+            want = oracle_mod.fill_splitmix(t * RB, RB, 0).tobytes()
+            assert xor_bytes(shares[0][6 + j], shares[1][6 + j]) == want
+    finally:
+        acc.close()
