@@ -8,7 +8,8 @@ size-independent properties (tolerance: bit-exact):
   * the keys' shares over a 2^20-row window deep in the domain equal the
     oracle's scan of the same window at the same logical rows;
   * with a 2^28 x 64 B accounts table resident beside it, one pass over both
-    tables reconstructs every target row of both."""
+    tables reconstructs every target row of both;
+  * a batched pass of 16 queries (48 keys) reconstructs every target row."""
 import numpy as np
 import pytest
 
@@ -100,3 +101,20 @@ def test_full_size_mixed_tables_one_pass_reconstruct(scanner, oracle_mod, big):
             assert xor_bytes(shares[0][6 + j], shares[1][6 + j]) == want
     finally:
         acc.close()
+
+
+def test_full_size_batched_pass_reconstructs(scanner, oracle_mod, big):
+    """16 queries (48 keys, one key group each) in one pass over the
+    2^31 x 32 B table, replayed from a CUDA graph: every share pair XORs to
+    its target row."""
+    targets = [int(x) for x in np.random.default_rng(7).integers(0, ROWS, 48)]
+    pairs = [oracle_keypair(oracle_mod, D, t, seed=37, i=j) for j, t in enumerate(targets)]
+    shares = []
+    for side in (0, 1):
+        ws = scanner.workspace()
+        ws.set_keys([big] * 48, [p[side] for p in pairs])
+        ws.launch(graph=True)
+        shares.append(ws.read())
+        ws.close()
+    for j, t in enumerate(targets):
+        assert xor_bytes(shares[0][j], shares[1][j]) == oracle_mod.fill_splitmix(t * RB, RB, 0).tobytes()
